@@ -1,0 +1,471 @@
+"""Benchmark: batched uneven breast-MIMO 2D FDTD + DAS on B200.
+
+Workload (one bench "step"): 64 seeded breast phantoms (sides drawn from
+{150,200,256,384,512}, dx = 0.5 mm, Courant 0.5), each with a 16-antenna
+ring; every transmitter is a separate 3000-step solve recording 16 receivers,
+for the tumour phantom AND its healthy twin (2 x 1024 solves, each batch one
+persistent launch), followed by one 128x128 DAS image per phantom of
+S_tumour - S_healthy.  Metric: aggregate Gcell-updates/s (cells x steps of all
+solves / time).  Inputs (fields 2 x 1.3 GB) are far larger than L2, so no L2
+flush is needed between steps.
+
+Legs reported on one JSON line:
+  value      device-resident, CUDA-event timed, max over ranks (replicas per GPU)
+  e2e        same work through the public API from pinned HOST buffers: H2D of
+             coefficients/waveforms and D2H of all traces and images inside
+             the timed region
+  plain_per_solve  the same solves one wf_fdtd2d_run at a time (measured on a
+             stratified sample, one phantom per grid size, extrapolated)
+  roofline   k_batch2d: 32 algorithmic bytes per cell-update / launch time
+  cpu_baseline  the CPU port of the reference loop (oracle) on a bounded sample
+`--impl reference` runs only the reference CPU port (rank 0) on the same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "batched Gcell-upd/s (uneven breast MIMO, 2D TM lossy fp32)"
+UNIT = "Gcell-upd/s"
+BYTES_PER_CELL_UPDATE = 32  # read Ex,Ey,Hz,Ca,Cb + write Ex,Ey,Hz (float32)
+DAS_SIZE = 128
+EPS_EFF = 0.6 * 5.0 + 0.3 * 40.0 + 0.1 * 36.0  # breast volume-weighted average
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def build_workload(dev, n_phantoms, n_tx, steps, seed):
+    from waveforge_b200 import (Batch2D, BatchSolve, Detectors, PointSource, SourceCollection,
+                                YeeGrid)
+    from waveforge_b200.core.materials import Material, MaterialMap
+    from waveforge_b200.core.sources import GaussianDerivativePulse
+    from waveforge_b200 import workloads as W
+
+    wl = W.BreastMIMO(n_phantoms=n_phantoms, n_tx=n_tx, steps=steps, seed=seed)
+    phantoms = wl.phantoms()
+    host_coeffs = {}   # (p, twin) -> (ca, cb) pinned host
+    dev_coeffs = {}
+    waves = {}
+    solves = {True: [], False: []}
+    for p, ph in enumerate(phantoms):
+        gh = YeeGrid(ph.side, ph.side, wl.dx, wl.dx, courant=wl.courant, device="cpu")
+        g = YeeGrid(ph.side, ph.side, wl.dx, wl.dx, courant=wl.courant, device=dev)
+        if ph.side not in waves:
+            waves[ph.side] = GaussianDerivativePulse(1e9).build(steps, g.dt, dev)
+        ant = ph.antennas(16)
+        for tumor in (True, False):
+            mm = MaterialMap(gh, default=ph.background(Material))
+            ph.paint(mm, Material, with_tumor=tumor)
+            ca, cb = mm.build()
+            host_coeffs[(p, tumor)] = (ca.pin_memory(), cb.pin_memory())
+            cad, cbd = ca.to(dev), cb.to(dev)
+            dev_coeffs[(p, tumor)] = (cad, cbd)
+            for tx in range(n_tx):
+                i, j = ant[tx]
+                src = PointSource(_TableWave(waves[ph.side]), i, j, "Hz", grid=g, N_steps=steps)
+                solves[tumor].append(BatchSolve(g, SourceCollection([src]), Detectors(ant), cad, cbd,
+                                                tag=(p, tx)))
+    batches = {t: Batch2D(solves[t], steps) for t in (True, False)}
+    return wl, phantoms, batches, host_coeffs, dev_coeffs, waves
+
+
+class _TableWave:
+    """Waveform already on the device (shared by all solves of one grid size)."""
+
+    def __init__(self, t):
+        self.t = t
+
+    def build(self, N_steps, dt, device, dtype=torch.float32):
+        return self.t[:N_steps]
+
+
+def das_all(batches, phantoms, wl, n_tx, dev, out_images):
+    from waveforge_b200.imaging.das import das_image_device, pixel_axes
+    v = 299_792_458.0 / math.sqrt(EPS_EFF)
+    for p, ph in enumerate(phantoms):
+        q0 = p * n_tx
+        tr_t = batches[True].traces_block(q0, n_tx)
+        tr_h = batches[False].traces_block(q0, n_tx)
+        ant = ph.antennas(16)
+        ax = torch.tensor([a[0] * wl.dx for a in ant], dtype=torch.float64)
+        ay = torch.tensor([a[1] * wl.dx for a in ant], dtype=torch.float64)
+        px, py = pixel_axes(ph.side, ph.side, wl.dx, (DAS_SIZE, DAS_SIZE))
+        dt = batches[True].solves[q0].grid.dt
+        das_image_device(tr_t, ax, ay, torch.from_numpy(px), torch.from_numpy(py), v, dt,
+                         out=out_images[p], traces_ref=tr_h)
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            out_dir = ROOT / "gpurun_out"
+            out_dir.mkdir(exist_ok=True)
+            self.path = out_dir / f"clocks_gpu{self.gpu}.csv"
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except Exception:  # nvidia-smi absent: report no clock record
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference port (oracle) timing
+# ---------------------------------------------------------------------------
+
+def cpu_reference_sample(budget_s=12.0, threads=None):
+    """Time the CPU port of the reference 2D loop on solves of the workload
+    until ``budget_s`` of work; returns (Gcell-upd/s, cores, sample text)."""
+    import oracle
+    from waveforge_b200 import workloads as W
+    from waveforge_b200.core.grid import YeeGrid
+    from waveforge_b200.core.materials import Material, MaterialMap
+
+    threads = threads or os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    wl = W.BreastMIMO()
+    phantoms = wl.phantoms()
+    done_cells = 0
+    t_total = 0.0
+    solves = 0
+    steps_each = 300
+    for ph in phantoms:
+        g = YeeGrid(ph.side, ph.side, wl.dx, wl.dx, courant=wl.courant, device="cpu")
+        mm = MaterialMap(g, default=ph.background(Material))
+        ph.paint(mm, Material)
+        ca, cb = mm.build()
+        ant = ph.antennas(16)
+        o = oracle.Oracle2D(ph.side, ph.side, wl.dx, wl.dx, g.dt, ca[..., 0], cb[..., 0])
+        o.add_point_source("Hz", *ant[0], oracle.gauss_deriv_wave(steps_each, g.dt))
+        t0 = time.perf_counter()
+        o.run(steps_each, [("Hz", i, j) for i, j in ant])
+        t_total += time.perf_counter() - t0
+        done_cells += ph.side * ph.side * steps_each
+        solves += 1
+        if t_total >= budget_s:
+            break
+    return (done_cells / t_total / 1e9, threads,
+            f"{solves} solves of the workload (first phantoms, TX 0), {steps_each} steps each, "
+            f"16 receivers gathered per step; {done_cells:.3e} cell-updates in {t_total:.1f} s")
+
+
+# ---------------------------------------------------------------------------
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def reduce_max(x, ws, dev):
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    t0 = time.perf_counter()
+    vals = []
+    samples = ""
+    for s in range(args.warmup + args.steps):
+        v, cores, samples = cpu_reference_sample(budget_s=args.ref_budget)
+        if s >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "breast_mimo_64ph_16tx_3000steps", "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": samples},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.perf_counter() - t0}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--phantoms", type=int, default=64)
+    ap.add_argument("--tx", type=int, default=16)
+    ap.add_argument("--nsteps", type=int, default=3000)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--ref-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, ws, rank)
+        barrier(ws)
+        return
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t_setup = time.perf_counter()
+    wl, phantoms, batches, host_coeffs, dev_coeffs, waves = build_workload(
+        dev, args.phantoms, args.tx, args.nsteps, args.seed)
+    images = torch.zeros((len(phantoms), DAS_SIZE, DAS_SIZE), dtype=torch.float64, device=dev)
+    cells_per_step = 2 * batches[True].cells * args.nsteps   # both twins
+    log(f"[bench] setup {time.perf_counter() - t_setup:.1f}s, {2 * len(batches[True].solves)} solves, "
+        f"{cells_per_step:.3e} cell-updates per step")
+    stream = torch.cuda.current_stream(dev)
+
+    kern_ms = []
+
+    def one_step(record=False):
+        for b in batches.values():
+            b.reset()
+        ev = []
+        for t in (True, False):
+            b = batches[t]
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            b._upload(0, args.nsteps)
+            e0.record(stream)
+            b.launch()
+            e1.record(stream)
+            b.step = args.nsteps
+            ev.append((e0, e1))
+        das_all(batches, phantoms, wl, args.tx, dev, images)
+        return ev
+
+    # ---- device-resident leg -------------------------------------------
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clk = ClockSampler(local)
+    clk.start()
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    evs = []
+    for _ in range(args.steps):
+        evs.append(one_step())
+    end.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clocks = clk.stop()
+    ms_total = start.elapsed_time(end)
+    for ev in evs:
+        for e0, e1 in ev:
+            kern_ms.append(e0.elapsed_time(e1))
+    statuses = batches[True].statuses() + batches[False].statuses()
+    if any(statuses):
+        raise RuntimeError(f"batched solves reported status {set(statuses)}")
+    ms_total = reduce_max(ms_total, ws, dev)
+    ms_step = ms_total / args.steps
+    value = ws * cells_per_step / (ms_step * 1e-3) / 1e9
+
+    # ---- e2e leg: host buffers through the public API ---------------------
+    host_traces = {t: torch.empty(batches[t]._traces.shape, dtype=torch.float32, pin_memory=True)
+                   for t in batches}
+    host_images = torch.empty(images.shape, dtype=torch.float64, pin_memory=True)
+    h2d = sum(c.numel() * 4 * 2 for c, _ in host_coeffs.values()) + sum(
+        w.numel() * 4 for w in waves.values())
+    d2h = sum(h.numel() * 4 for h in host_traces.values()) + host_images.numel() * 8
+    host_waves = {k: w.cpu().pin_memory() for k, w in waves.items()}
+
+    def e2e_step():
+        for key, (ca_h, cb_h) in host_coeffs.items():
+            ca_d, cb_d = dev_coeffs[key]
+            ca_d.copy_(ca_h, non_blocking=True)
+            cb_d.copy_(cb_h, non_blocking=True)
+        for k, w in host_waves.items():
+            waves[k].copy_(w, non_blocking=True)
+        one_step()
+        for t in batches:
+            host_traces[t].copy_(batches[t]._traces, non_blocking=True)
+        host_images.copy_(images, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    s2 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e2.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    ms_e2e = reduce_max(s2.elapsed_time(e2), ws, dev) / args.steps
+    e2e_value = ws * cells_per_step / (ms_e2e * 1e-3) / 1e9
+
+    # ---- plain per-solve comparison (stratified sample) -------------------
+    plain = None
+    if not args.no_plain:
+        by_side = {}
+        for p, ph in enumerate(phantoms):
+            by_side.setdefault(ph.side, p)
+        counts = {}
+        for ph in phantoms:
+            counts[ph.side] = counts.get(ph.side, 0) + 1
+        sub_solves = []
+        for side, p in sorted(by_side.items()):
+            sub_solves += [batches[True].solves[p * args.tx + tx] for tx in range(2)]
+        from waveforge_b200 import Batch2D
+        sub = Batch2D(sub_solves, args.nsteps)
+        per_side_ms = {}
+        for q in range(0, len(sub_solves), 2):
+            side = sub_solves[q].grid.Nx
+            times = []
+            for rep in range(2):
+                sub.reset()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                sub.run_plain_one(q)
+                b.record(stream)
+                torch.cuda.synchronize(dev)
+                times.append(a.elapsed_time(b))
+            per_side_ms[side] = min(times)
+        total_ms = sum(counts[s] * args.tx * per_side_ms[s] for s in counts) * 2  # both twins
+        plain_value = cells_per_step / (total_ms * 1e-3) / 1e9
+        plain = {"value": plain_value, "unit": UNIT,
+                 "ms_per_solve_by_side": {str(k): round(v, 3) for k, v in sorted(per_side_ms.items())},
+                 "sample": "one phantom per grid size, 2 TX each, timed one solve at a time with "
+                           "wf_fdtd2d_run; extrapolated by the workload's size histogram",
+                 "batched_over_plain": value / ws / plain_value}
+
+    # ---- roofline of the dominant kernel ----------------------------------
+    peak, peak_kind = measured_peaks()
+    k_ms = statistics.mean(kern_ms)
+    achieved = BYTES_PER_CELL_UPDATE * (cells_per_step / 2) / (k_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "k_batch2d_traffic.txt"
+    if tfile.exists():
+        for line in tfile.read_text().splitlines():
+            if line.startswith("dram_bytes_per_cell_update="):
+                traffic = float(line.split("=")[1]) * cells_per_step / 2
+    roof = {"bound": "hbm", "kernel": "k_batch2d", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+            "bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
+            "launch_ms": k_ms, "note": "algorithmic bytes = 32 B x cell-updates of one launch; "
+                                       "temporal blocking re-uses tiles on chip, so frac may exceed 1"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_reference_sample()
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"breast_mimo_{len(phantoms)}ph_{args.tx}tx_{args.nsteps}steps",
+                       "solves_per_step": 2 * len(batches[True].solves),
+                       "twins": "tumour + healthy", "das": f"{len(phantoms)} x {DAS_SIZE}x{DAS_SIZE}",
+                       "cell_updates_per_step": cells_per_step, "grid_sides": "150-512",
+                       "dx_mm": 0.5, "courant": 0.5, "l2": "inputs > L2 (2.6 GB fields), no flush",
+                       "parallelism": f"replicas x{ws}"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+            "plain_per_solve": plain, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": args.steps * (2 + len(phantoms)),
+        }
+        print(json.dumps(line), flush=True)
+    barrier(ws)
+
+
+if __name__ == "__main__":
+    main()

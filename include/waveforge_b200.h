@@ -1,0 +1,194 @@
+/*
+ * waveforge_b200.h -- C ABI of the B200 (sm_100a) Yee-FDTD + DAS engine.
+ *
+ * The reference project (shahzaibshazoo/waveforge) is pure Python/PyTorch and
+ * has no native interface; each entry point below replaces one Python call
+ * path of the reference, cited next to it.  All pointers are DEVICE pointers
+ * unless marked "host"; sizes are element counts; streams are cudaStream_t
+ * passed as void*.  Every function returns 0 on success or a WF_E* code and
+ * never aborts or traps; wf_last_error() gives a message for the calling
+ * thread.  The library allocates no device memory on these paths: scratch
+ * buffers (ping-pong partners, work queues) are passed in by the caller.
+ *
+ * Field layout: row-major (i, j[, k]) with the LAST index unit-stride, exactly
+ * the layout of the reference FieldSet tensors (src/core/fields.py:156-168,
+ * 2D tensors are (Nx, Ny, 1)).  Component codes follow
+ * src/core/fields.py:24 FIELD_COMPONENTS order.
+ */
+#ifndef WAVEFORGE_B200_H
+#define WAVEFORGE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WF_ABI_VERSION 1
+
+/* status codes */
+#define WF_OK            0
+#define WF_E_ARG         1   /* bad argument (size, pointer, range) */
+#define WF_E_CUDA        2   /* a CUDA runtime call failed */
+#define WF_E_LIMIT       3   /* a compile-time capacity was exceeded */
+#define WF_E_DIVERGED    4   /* stability threshold exceeded (host-side check) */
+#define WF_E_TIMEOUT     5   /* a bounded device wait gave up */
+
+/* field component codes, src/core/fields.py:24 */
+#define WF_EX 0
+#define WF_EY 1
+#define WF_EZ 2
+#define WF_HX 3
+#define WF_HY 4
+#define WF_HZ 5
+
+/* 2D TM grid constants, all float32-rounded exactly as PyTorch rounds the
+ * Python-float scalars of the reference update (src/core/fdtd2d.py:158-161,
+ * src/core/boundaries.py:177-178). */
+typedef struct wf_grid2d {
+  int32_t nx, ny;
+  float dh;      /* dt / MU0 */
+  float de;      /* dt / EPS0 (vacuum scalar path) */
+  float dx, dy;
+  float mur_x, mur_y;
+} wf_grid2d;
+
+/* 3D grid constants (src/core/fdtd3d.py:206-211, boundaries.py:429-431). */
+typedef struct wf_grid3d {
+  int32_t nx, ny, nz;
+  float dh, de;
+  float dx, dy, dz;
+  float mur_x, mur_y, mur_z;
+} wf_grid3d;
+
+/* One soft source (src/core/sources.py: PointSource :863-887, LineSource
+ * :1015-1035, PlaneSource :730-749).  Every cell of the half-open box
+ * [i0,i1)x[j0,j1)x[k0,k1) of component `comp` gets, at step n (before the H
+ * update), field += wave[n] (amp == NULL) or field += wave[n]*amp[c] where c
+ * is the row-major offset of the cell inside the box.  Sources are applied in
+ * array order, as SourceCollection.step does (:1060-1071). */
+typedef struct wf_source {
+  int32_t comp;
+  int32_t i0, i1, j0, j1, k0, k1;
+  int32_t n_wave;
+  const float* wave;
+  const float* amp;
+} wf_source;
+
+/* One detector sample point: records comp[i,j,k] after every full step
+ * (examples/brain_mimo_imaging.py:193-201). */
+typedef struct wf_probe {
+  int32_t comp, i, j, k;
+} wf_probe;
+
+/* Launch shape of the temporally blocked kernels. steps_per_pass = temporal
+ * block depth K; tile_i x tile_j (x tile_k) = core cells written per CTA. */
+typedef struct wf_tune {
+  int32_t steps_per_pass;
+  int32_t tile_i, tile_j, tile_k;
+  int32_t threads;
+} wf_tune;
+
+/* Library identity and the last error message of the calling thread. */
+int32_t     wf_abi_version(void);
+const char* wf_last_error(void);
+
+/* Advance a 2D TM grid nsteps time steps.
+ * Replaces FDTD2D.step/run (src/core/fdtd2d.py:187-359) together with
+ * MurABC.snapshot/apply (src/core/boundaries.py:230-274), the source
+ * injection of SourceCollection.step (src/core/sources.py:1060-1071) and the
+ * per-step detector gather (examples/brain_mimo_imaging.py:193-201).
+ *
+ *  ex,ey,hz     state, nx*ny each, updated in place (result always lands here)
+ *  sx,sy,sz     caller-owned scratch, nx*ny each (ping-pong partner)
+ *  ca,cb        per-cell coefficients nx*ny each, or both NULL (vacuum path)
+ *  src,nsrc     device array of sources; every wave must have n_wave > last step
+ *  probes,nprobe  device array of detector points
+ *  traces       nprobe rows of trace_ld floats; step n goes to column n-trace_step0
+ *  step0        global index of the first step (waveform row, trace column)
+ *  n_check      stability-check period (steps_completed % n_check == 0)
+ *  check_max    per-check maxima of |Ex|,|Ey|,|Hz| as float bits, 3 per check,
+ *               indexed by (n+1)/n_check - (step0/n_check) - 1; NULL = off.
+ *               The caller zeroes it.
+ *  tune         NULL = built-in default.
+ */
+int32_t wf_fdtd2d_run(const wf_grid2d* g,
+                      float* ex, float* ey, float* hz,
+                      float* sx, float* sy, float* sz,
+                      const float* ca, const float* cb,
+                      const wf_source* src, int32_t nsrc,
+                      const wf_probe* probes, int32_t nprobe,
+                      float* traces, int64_t trace_ld, int32_t trace_step0,
+                      int32_t step0, int32_t nsteps,
+                      int32_t n_check, uint32_t* check_max,
+                      const wf_tune* tune, void* stream);
+
+/* Advance a 3D grid nsteps time steps.
+ * Replaces FDTD3D.step/run (src/core/fdtd3d.py:261-516) with
+ * MurABC3D.snapshot/apply (src/core/boundaries.py:488-583), source injection
+ * and detector gather.  f[6] = Ex,Ey,Ez,Hx,Hy,Hz state (nx*ny*nz each);
+ * s[6] = scratch partners; check_max holds 6 maxima per check. */
+int32_t wf_fdtd3d_run(const wf_grid3d* g,
+                      float* const* f, float* const* s,
+                      const float* ca, const float* cb,
+                      const wf_source* src, int32_t nsrc,
+                      const wf_probe* probes, int32_t nprobe,
+                      float* traces, int64_t trace_ld, int32_t trace_step0,
+                      int32_t step0, int32_t nsteps,
+                      int32_t n_check, uint32_t* check_max,
+                      const wf_tune* tune, void* stream);
+
+/* One solve of a batched launch: an independent 2D TM grid with its own
+ * state, scratch, coefficients, sources, probes and trace buffer.
+ * Batching many of these is new functionality: the reference runs MIMO
+ * transmitters one FDTD2D at a time (examples/brain_mimo_imaging.py:176-204,
+ * examples/10_breast_tumor_mimo.py:123-145). */
+typedef struct wf_solve2d {
+  wf_grid2d g;
+  float *ex, *ey, *hz;
+  float *sx, *sy, *sz;
+  const float *ca, *cb;
+  const wf_source* src;
+  const wf_probe* probes;
+  float* traces;
+  int64_t trace_ld;
+  int32_t nsrc, nprobe;
+  int32_t trace_step0;
+  int32_t step0, nsteps;      /* steps to advance in this launch */
+  int32_t n_check;            /* stability-check period, as in wf_fdtd2d_run */
+  int32_t status;             /* written by the device: 0 ok, else WF_E_* */
+  uint32_t* check_max;        /* 3 maxima per check, or NULL */
+} wf_solve2d;
+
+/* Advance every solve of a device array of descriptors in ONE persistent
+ * launch: resident CTAs pull solves from a device work queue (queue[0] is the
+ * next-item counter, zeroed by the caller; order[] lists solve indices,
+ * largest first) and run each through all its steps with the same tile
+ * routine as wf_fdtd2d_run, so each solve's result is bit-identical to
+ * running it alone.  Each solve's result lands in its ex/ey/hz. */
+int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve,
+                       const int32_t* order, int32_t* queue,
+                       const wf_tune* tune, int32_t ctas_per_sm, void* stream);
+
+/* Delay-and-sum backprojection on the device, bit-identical to the reference
+ * NumPy float64 path of examples/brain_mimo_imaging.py:211-266 (and its
+ * variants through px/py, gate_start, skip_self).
+ *  traces   (nant, nant, n_steps) float32, [tx][rx][n]
+ *  traces_ref  NULL, or a second array of the same shape: the samples are then
+ *           traces - traces_ref in float32 (delta_S = S_tumor - S_healthy,
+ *           examples/brain_mimo_imaging.py:314)
+ *  ant_x/y  nant antenna coordinates in metres (float64)
+ *  px, py   nxi / nyi pixel coordinates in metres (float64)
+ *  image    nxi*nyi float64 output, row-major [ix][iy], squared sum. */
+int32_t wf_das2d(const float* traces, const float* traces_ref, int32_t nant, int32_t n_steps,
+                 const double* ant_x, const double* ant_y,
+                 const double* px, int32_t nxi, const double* py, int32_t nyi,
+                 double v_medium, double dt,
+                 int32_t gate_start, int32_t skip_self,
+                 double* image, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WAVEFORGE_B200_H */

@@ -1,0 +1,448 @@
+"""Generate the golden vectors of the parity tests by running the REFERENCE.
+
+Run in a container that holds the read-only reference checkout:
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+It imports the reference's own ``core`` package and example DAS functions
+(pure Python + PyTorch, CPU), runs each case in float32 and float64, and
+writes ``tests/golden/<case>.npz`` with:
+  * the exact inputs the product needs to rebuild the case (waveform table,
+    source / receiver positions, grid constants),
+  * SHA-256 digests of the float32 outputs (traces, final fields, Ca/Cb),
+    so tests can demand bit-identical results,
+  * decimated float32 and float64 samples of the same outputs for
+    relative-L2 error statements.
+Nothing on the GPU box reads the reference; only these fixtures travel.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import importlib.util
+import math
+import sys
+import warnings
+from pathlib import Path
+
+import numpy as np
+import torch
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+from waveforge_b200 import workloads as W  # noqa: E402  (recipes only; no compute)
+
+warnings.filterwarnings("ignore", category=UserWarning)
+
+
+def sha(t) -> str:
+    a = t.detach().cpu().contiguous().numpy() if torch.is_tensor(t) else np.ascontiguousarray(t)
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+def load_ref(ref: Path):
+    sys.path.insert(0, str(ref / "src"))
+    import core  # noqa: F401  the reference package
+    from core import grid, fields, materials, sources, boundaries, fdtd2d, fdtd3d
+    return dict(grid=grid, fields=fields, materials=materials, sources=sources,
+                boundaries=boundaries, fdtd2d=fdtd2d, fdtd3d=fdtd3d)
+
+
+def load_example(ref: Path, rel: str, name: str):
+    spec = importlib.util.spec_from_file_location(name, ref / "examples" / rel)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def gauss_deriv_class(R):
+    Waveform = R["sources"].Waveform
+
+    class GaussDeriv(Waveform):
+        """Benchmark pulse on the reference Waveform base (same expression as
+        waveforge_b200.core.sources.GaussianDerivativePulse)."""
+
+        def __init__(self, fc=1e9, amplitude=1.0):
+            self.fc, self.A = fc, amplitude
+            self.tau = 1.0 / (2.0 * math.pi * fc)
+            self.t0 = 3.0 * self.tau
+
+        def _compute(self, t):
+            u = (t - self.t0) / self.tau
+            return self.A * (-u) * torch.exp(-0.5 * (u * u))
+
+        peak_time = property(lambda s: s.t0 - s.tau)
+        bandwidth = property(lambda s: s.fc)
+        amplitude = property(lambda s: s.A)
+
+    return GaussDeriv
+
+
+def run_2d(R, nx, ny, dx, courant, steps, dtype, paint=None, default=None, sources=(), probes=(),
+           n_check=10 ** 9):
+    """sources: (comp, kind, args, wave_tensor) ; probes: (comp, i, j)."""
+    grid = R["grid"].YeeGrid(nx, ny, dx, dx, courant=courant, device="cpu", dtype=dtype)
+    f = R["fields"].FieldSet(grid)
+    b = R["boundaries"].MurABC(grid, f.Hz)
+    Ca = Cb = None
+    if paint is not None:
+        mm = R["materials"].MaterialMap(grid, default=default)
+        paint(mm, R["materials"].Material)
+        Ca, Cb = mm.build()
+    TW = tab_class(R)
+    srcs = []
+    for comp, kind, args, wave in sources:
+        w = TW(wave)
+        if kind == "point":
+            srcs.append(R["sources"].PointSource(w, *args, comp, grid=grid, N_steps=steps))
+        elif kind == "line":
+            axis, pos, start, stop, amp = args
+            srcs.append(R["sources"].LineSource(w, axis, pos, start, stop, comp, grid=grid,
+                                                N_steps=steps, amplitude_profile=amp))
+    sc = R["sources"].SourceCollection(srcs) if srcs else None
+    sim = R["fdtd2d"].FDTD2D(grid, f, b, sc, Ca=Ca, Cb=Cb, n_check=n_check)
+    tr = torch.zeros(len(probes), steps, dtype=dtype)
+    for s in range(steps):
+        sim.step()
+        for r, (comp, i, j) in enumerate(probes):
+            tr[r, s] = getattr(f, comp)[i, j, 0]
+    return grid, f, tr, Ca, Cb
+
+
+def tab_class(R):
+    Waveform = R["sources"].Waveform
+
+    class Tab(Waveform):
+        def __init__(self, table):
+            self.table = table
+
+        def build(self, N_steps, dt, device, dtype=torch.float32):
+            return self.table[:N_steps].to(dtype).to(device)
+
+        def _compute(self, t):
+            raise NotImplementedError
+
+        peak_time = property(lambda s: -1.0)
+        bandwidth = property(lambda s: 0.0)
+        amplitude = property(lambda s: 1.0)
+
+    return Tab
+
+
+def dec(a, k):
+    return np.ascontiguousarray(np.asarray(a)[..., ::k])
+
+
+def case_vacuum_point(R, out):
+    """256^2 vacuum, Hz point source at (128,128), 4 receivers at 60 cells, 1000 steps."""
+    GD = gauss_deriv_class(R)
+    n, steps = 256, 1000
+    rx = [("Hz", 188, 128), ("Hz", 128, 188), ("Hz", 68, 128), ("Hz", 128, 68)]
+    res = {}
+    for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+        grid = R["grid"].YeeGrid(n, n, 1e-3, 1e-3, courant=0.5, device="cpu", dtype=dtype)
+        wave = GD().build(steps, grid.dt, torch.device("cpu"), dtype)
+        if dtype == torch.float32:
+            wave32 = wave.clone()
+        g, f, tr, _, _ = run_2d(R, n, n, 1e-3, 0.5, steps, dtype,
+                                sources=[("Hz", "point", (128, 128), wave)], probes=rx)
+        res[dt_name] = (g, f, tr)
+    g32, f32, tr32 = res["32"]
+    _, f64, tr64 = res["64"]
+    np.savez_compressed(
+        out / "vacuum_point_256.npz", n=n, steps=steps, dx=1e-3, courant=0.5, dt=g32.dt,
+        src=np.array([128, 128]), rx=np.array([r[1:] for r in rx]), wave=wave32.numpy(),
+        traces32=tr32.numpy(), traces64=tr64.numpy(),
+        sha_traces=sha(tr32), sha_ex=sha(f32.Ex), sha_ey=sha(f32.Ey), sha_hz=sha(f32.Hz),
+        hz32=f32.Hz[..., 0].numpy(), hz64_dec=dec(f64.Hz[::2, :, 0].numpy(), 2))
+
+
+def case_lossy_ellipses(R, out, n=256, steps=600):
+    wl = W.LossyEllipses(n=n, steps=steps)
+    GD = gauss_deriv_class(R)
+    M = R["materials"].Material
+    rx = [("Hz", i, j) for i, j in wl.receivers]
+    res = {}
+    for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+        grid = R["grid"].YeeGrid(n, n, wl.dx, wl.dx, courant=wl.courant, device="cpu", dtype=dtype)
+        wave = GD().build(steps, grid.dt, torch.device("cpu"), dtype)
+        if dtype == torch.float32:
+            wave32 = wave.clone()
+        res[dt_name] = run_2d(R, n, n, wl.dx, wl.courant, steps, dtype, paint=wl.paint,
+                              default=wl.background(M),
+                              sources=[("Hz", "point", wl.source, wave)], probes=rx)
+    g32, f32, tr32, ca, cb = res["32"]
+    _, f64, tr64, _, _ = res["64"]
+    np.savez_compressed(
+        out / f"lossy_ellipses_{n}.npz", n=n, steps=steps, dx=wl.dx, courant=wl.courant,
+        dt=g32.dt, seed=wl.seed, src=np.array(wl.source), rx=np.array([r[1:] for r in rx]),
+        wave=wave32.numpy(), sha_ca=sha(ca), sha_cb=sha(cb), traces32=tr32.numpy(),
+        traces64=tr64.numpy(), sha_traces=sha(tr32), sha_ex=sha(f32.Ex), sha_ey=sha(f32.Ey),
+        sha_hz=sha(f32.Hz), hz32_dec=dec(f32.Hz[::4, :, 0].numpy(), 4),
+        hz64_dec=dec(f64.Hz[::4, :, 0].numpy(), 4))
+
+
+def case_breast_mimo(R, out, sides=(150, 200), n_tx=2, steps=1500):
+    """Two breast phantoms (fixed sides), first n_tx transmitters each, 16 receivers."""
+    wl = W.BreastMIMO(n_phantoms=len(sides), steps=steps)
+    rng = np.random.default_rng(wl.seed)
+    phantoms = [W.BreastPhantom.draw(rng, side=s) for s in sides]
+    GD = gauss_deriv_class(R)
+    M = R["materials"].Material
+    data = dict(steps=steps, dx=wl.dx, courant=wl.courant, seed=wl.seed, sides=np.array(sides),
+                n_tx=n_tx)
+    for p_idx, ph in enumerate(phantoms):
+        ant = ph.antennas(16)
+        rx = [("Hz", i, j) for i, j in ant]
+        data[f"p{p_idx}_geom"] = np.array([ph.side, ph.A, ph.B, *ph.tumor_center, ph.tumor_r])
+        data[f"p{p_idx}_ant"] = np.array(ant)
+        for tx in range(n_tx):
+            res = {}
+            for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+                grid = R["grid"].YeeGrid(ph.side, ph.side, wl.dx, wl.dx, courant=wl.courant,
+                                         device="cpu", dtype=dtype)
+                wave = GD().build(steps, grid.dt, torch.device("cpu"), dtype)
+                if dtype == torch.float32:
+                    data["wave"] = wave.numpy()
+                    data["dt"] = grid.dt
+                res[dt_name] = run_2d(R, ph.side, ph.side, wl.dx, wl.courant, steps, dtype,
+                                      paint=lambda mm, Mat, ph=ph: ph.paint(mm, Mat),
+                                      default=ph.background(M),
+                                      sources=[("Hz", "point", ant[tx], wave)], probes=rx)
+            _, f32, tr32, ca, cb = res["32"]
+            _, f64, tr64, _, _ = res["64"]
+            key = f"p{p_idx}_tx{tx}"
+            data[key + "_sha_traces"] = sha(tr32)
+            data[key + "_sha_hz"] = sha(f32.Hz)
+            data[key + "_traces32_dec"] = dec(tr32.numpy(), 5)
+            data[key + "_traces64_dec"] = dec(tr64.numpy(), 5)
+            data[f"p{p_idx}_sha_ca"] = sha(ca)
+            data[f"p{p_idx}_sha_cb"] = sha(cb)
+    np.savez_compressed(out / "breast_mimo_small.npz", **data)
+
+
+def case_edges_2d(R, out):
+    """Tiny grids exercising edge semantics: sources on edges/corners, E
+    sources, overlapping sources, a weighted line source, odd sizes."""
+    rng = np.random.default_rng(11)
+    cases = {}
+    specs = [
+        ("tiny7x5", 7, 5, 60, None,
+         [("Hz", "point", (0, 0)), ("Hz", "point", (1, 1)), ("Ex", "point", (3, 0)),
+          ("Ey", "point", (0, 2)), ("Hz", "line", ("x", 4, 0, 7, True)),
+          ("Hz", "point", (6, 4)), ("Hz", "point", (6, 4)), ("Hz", "point", (1, 3))]),
+        ("odd33x17", 33, 17, 150, "circles",
+         [("Hz", "point", (1, 8)), ("Hz", "point", (32, 16)), ("Ey", "line", ("y", 20, 2, 15, False))]),
+        ("min4x4", 4, 4, 40, None, [("Hz", "point", (1, 2)), ("Ex", "point", (2, 1))]),
+    ]
+    for name, nx, ny, steps, mat, srcs in specs:
+        waves = [torch.from_numpy(rng.standard_normal(steps).astype(np.float32)) for _ in srcs]
+        amps = {}
+        full = []
+        for q, ((comp, kind, args), w) in enumerate(zip(srcs, waves)):
+            if kind == "line":
+                axis, pos, start, stop, weighted = args
+                amp = (torch.from_numpy(rng.uniform(0.5, 2.0, stop - start).astype(np.float32))
+                       if weighted else None)
+                amps[q] = amp
+                full.append((comp, "line", (axis, pos, start, stop, amp), w))
+            else:
+                full.append((comp, "point", args, w))
+        probes = [(c, i, j) for c in ("Ex", "Ey", "Hz") for i in range(nx) for j in range(ny)
+                  if (i in (0, 1, nx - 2, nx - 1) or j in (0, 1, ny - 2, ny - 1))][:200]
+        paint = None
+        default = None
+        if mat == "circles":
+            M = R["materials"].Material
+            default = M("bg", 4.0, 0.1)
+            circ = [(float(a), float(b), float(c), float(e), float(s)) for a, b, c, e, s in
+                    zip(rng.uniform(0, nx, 4), rng.uniform(0, ny, 4), rng.uniform(2, 8, 4),
+                        rng.uniform(1, 50, 4), rng.uniform(0, 2, 4))]
+
+            def paint(mm, Mat, circ=circ):
+                for q, (ci, cj, r, e, s) in enumerate(circ):
+                    mm.add_circle((ci, cj), r, Mat(f"c{q}", e, s))
+        for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+            ws = [(c, k, a if k == "point" else (a[0], a[1], a[2], a[3], None if a[4] is None
+                   else a[4].to(dtype)), w.to(dtype)) for c, k, a, w in full]
+            g, f, tr, ca, cb = run_2d(R, nx, ny, 1e-3, 0.7, steps, dtype, paint=paint,
+                                      default=default, sources=ws, probes=probes)
+            if dtype == torch.float32:
+                d = dict(nx=nx, ny=ny, steps=steps, dx=1e-3, courant=0.7, dt=g.dt,
+                         ex32=f.Ex[..., 0].numpy(), ey32=f.Ey[..., 0].numpy(),
+                         hz32=f.Hz[..., 0].numpy(), traces32=tr.numpy(),
+                         probes=np.array([(("Ex", "Ey", "Hz").index(c), i, j) for c, i, j in probes]))
+                if ca is not None:
+                    d["ca"] = ca[..., 0].numpy()
+                    d["cb"] = cb[..., 0].numpy()
+                for q, ((comp, kind, args), w) in enumerate(zip(srcs, waves)):
+                    d[f"src{q}_comp"] = comp
+                    d[f"src{q}_kind"] = kind
+                    d[f"src{q}_args"] = np.array([v for v in (args if kind == "point" else args[1:4])])
+                    if kind == "line":
+                        d[f"src{q}_axis"] = args[0]
+                        if amps.get(q) is not None:
+                            d[f"src{q}_amp"] = amps[q].numpy()
+                    d[f"src{q}_wave"] = w.numpy()
+                d["nsrc"] = len(srcs)
+            else:
+                d["hz64"] = f.Hz[..., 0].numpy()
+        cases[name] = d
+    for name, d in cases.items():
+        np.savez_compressed(out / f"edges2d_{name}.npz", **d)
+
+
+def run_3d(R, shape, dx, courant, steps, dtype, paint=None, default=None, sources=(), probes=()):
+    nx, ny, nz = shape
+    grid = R["grid"].YeeGrid(nx, ny, dx, dx, Nz=nz, dz=dx, courant=courant, device="cpu", dtype=dtype)
+    f = R["fields"].FieldSet(grid)
+    b = R["boundaries"].MurABC3D(grid, f.Hx, f.Hy, f.Hz)
+    Ca = Cb = None
+    if paint is not None:
+        mm = R["materials"].MaterialMap3D(grid, default=default)
+        paint(mm, R["materials"].Material)
+        Ca, Cb = mm.build3d()
+    TW = tab_class(R)
+    srcs = []
+    for comp, kind, args, wave in sources:
+        w = TW(wave)
+        if kind == "point":
+            i, j, k = args
+            srcs.append(R["sources"].PointSource(w, i, j, comp, k=k, grid=grid, N_steps=steps))
+        elif kind == "plane":
+            plane, pos = args
+            srcs.append(R["sources"].PlaneSource(w, plane, pos, comp, grid=grid, N_steps=steps))
+    sc = R["sources"].SourceCollection(srcs) if srcs else None
+    sim = R["fdtd3d"].FDTD3D(grid, f, b, sc, Ca=Ca, Cb=Cb, n_check=10 ** 9)
+    tr = torch.zeros(len(probes), steps, dtype=dtype)
+    with torch.no_grad():
+        for s in range(steps):
+            sim.step()
+            for r, (comp, i, j, k) in enumerate(probes):
+                tr[r, s] = getattr(f, comp)[i, j, k]
+    return grid, f, tr, Ca, Cb
+
+
+def case_head3d(R, out, n=32, steps=200):
+    wl = W.Head3D(n=n, steps=steps)
+    GD = gauss_deriv_class(R)
+    M = R["materials"].Material
+    rx = [("Ez", *p) for p in wl.receivers()]
+    res = {}
+    for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+        dxx = wl.dx
+        stable = R["grid"].compute_stable_dt(dxx, dxx, dxx, wl.courant)
+        wave = GD().build(steps, stable, torch.device("cpu"), dtype)
+        if dtype == torch.float32:
+            wave32 = wave.clone()
+        res[dt_name] = run_3d(R, (n, n, n), dxx, wl.courant, steps, dtype, paint=wl.paint,
+                              default=wl.background(M),
+                              sources=[("Ez", "point", wl.source, wave)], probes=rx)
+    g, f32, tr32, ca, cb = res["32"]
+    _, f64, tr64, _, _ = res["64"]
+    np.savez_compressed(
+        out / f"head3d_{n}.npz", n=n, steps=steps, dx=wl.dx, courant=wl.courant, dt=g.dt,
+        seed=wl.seed, src=np.array(wl.source), rx=np.array([r[1:] for r in rx]),
+        wave=wave32.numpy(), sha_ca=sha(ca), sha_cb=sha(cb), traces32=tr32.numpy(),
+        traces64=tr64.numpy(), sha_traces=sha(tr32),
+        **{f"sha_{c.lower()}": sha(getattr(f32, c)) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
+
+
+def case_edges_3d(R, out):
+    rng = np.random.default_rng(12)
+    specs = [
+        ("box9x7x6", (9, 7, 6), 40, [("Hx", "point", (0, 3, 2)), ("Hy", "point", (4, 0, 5)),
+                                     ("Ez", "point", (4, 3, 0)), ("Hz", "point", (8, 6, 3)),
+                                     ("Ex", "plane", ("yz", 2)), ("Hz", "point", (1, 1, 1))]),
+        ("flat8x6x1", (8, 6, 1), 50, [("Hz", "point", (3, 2, 0)), ("Ez", "point", (5, 4, 0))]),
+    ]
+    for name, shape, steps, srcs in specs:
+        waves = [torch.from_numpy(rng.standard_normal(steps).astype(np.float32)) for _ in srcs]
+        nx, ny, nz = shape
+        probes = [(c, i, j, k) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+                  for i, j, k in [(0, 0, 0), (nx - 1, ny - 1, nz - 1), (1, 2, min(1, nz - 1)),
+                                  (nx // 2, ny // 2, nz // 2)]]
+        d = {}
+        for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+            ws = [(c, k, a, w.to(dtype)) for (c, k, a), w in zip(srcs, waves)]
+            g, f, tr, _, _ = run_3d(R, shape, 1e-3, 0.5, steps, dtype, sources=ws, probes=probes)
+            if dtype == torch.float32:
+                d.update(shape=np.array(shape), steps=steps, dx=1e-3, courant=0.5, dt=g.dt,
+                         traces32=tr.numpy(), nsrc=len(srcs),
+                         probes=np.array([(("Ex", "Ey", "Ez", "Hx", "Hy", "Hz").index(c), i, j, k)
+                                          for c, i, j, k in probes]))
+                for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+                    d[c.lower() + "32"] = getattr(f, c).numpy()
+                for q, ((comp, kind, args), w) in enumerate(zip(srcs, waves)):
+                    d[f"src{q}_comp"] = comp
+                    d[f"src{q}_kind"] = kind
+                    d[f"src{q}_args"] = np.array(args if kind == "point" else [("xy", "xz", "yz").index(args[0]), args[1]])
+                    d[f"src{q}_wave"] = w.numpy()
+            else:
+                d["hz64"] = f.Hz.numpy()
+        np.savez_compressed(out / f"edges3d_{name}.npz", **d)
+
+
+def case_das(R, ref: Path, out):
+    """DAS on a 96^2 breast-like phantom, 8 antennas, healthy vs tumour."""
+    bm = load_example(ref, "brain_mimo_imaging.py", "ref_brain_mimo")
+    bc = load_example(ref, "09_brain_clot_dataset_sample.py", "ref_brain_clot")
+    GD = gauss_deriv_class(R)
+    M = R["materials"].Material
+    side, steps = 96, 600
+    rng = np.random.default_rng(21)
+    ph = W.BreastPhantom.draw(rng, side=side)
+    ph = W.BreastPhantom(side, ph.A, ph.B, ph.tumor_center, max(6.0, ph.tumor_r / 2), ph.skin)
+    ant = ph.antennas(8)
+    grid = R["grid"].YeeGrid(side, side, 0.5e-3, 0.5e-3, courant=0.5, device="cpu")
+    wave = GD().build(steps, grid.dt, torch.device("cpu"), torch.float32)
+    S = {}
+    for tumor in (False, True):
+        sig = np.zeros((8, 8, steps), np.float32)
+        for tx in range(8):
+            _, _, tr, _, _ = run_2d(R, side, side, 0.5e-3, 0.5, steps, torch.float32,
+                                    paint=lambda mm, Mat, t=tumor: ph.paint(mm, Mat, with_tumor=t),
+                                    default=ph.background(M),
+                                    sources=[("Hz", "point", ant[tx], wave)],
+                                    probes=[("Hz", i, j) for i, j in ant])
+            sig[tx] = tr.numpy()
+        S[tumor] = sig
+    delta = S[True] - S[False]
+    img_c = bm.das_backprojection(delta, ant, grid, steps, image_shape=(48, 40))
+    img_f = bm.das_backprojection(delta, ant, grid, steps)
+    img_g = bc.das_backprojection(delta, ant, grid, steps)
+    np.savez_compressed(out / "das_breast96.npz", delta=delta, ant=np.array(ant), side=side,
+                        steps=steps, dx=0.5e-3, dt=grid.dt, img_canonical_48x40=img_c,
+                        img_full=img_f, img_gated=img_g, gate_start=max(0, int(0.9e-9 / grid.dt)),
+                        tumor=np.array([*ph.tumor_center, ph.tumor_r]))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default="")
+    a = ap.parse_args()
+    ref = Path(a.ref)
+    R = load_ref(ref)
+    torch.set_num_threads(8)
+    out = HERE
+    todo = {
+        "vacuum": lambda: case_vacuum_point(R, out),
+        "lossy": lambda: case_lossy_ellipses(R, out),
+        "breast": lambda: case_breast_mimo(R, out),
+        "edges2d": lambda: case_edges_2d(R, out),
+        "head3d": lambda: case_head3d(R, out),
+        "edges3d": lambda: case_edges_3d(R, out),
+        "das": lambda: case_das(R, ref, out),
+    }
+    for k, fn in todo.items():
+        if a.only and k not in a.only.split(","):
+            continue
+        print("golden:", k, flush=True)
+        fn()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,105 @@
+"""3D parity of the CUDA path with the reference: bit-identical float32
+traces and final fields (golden digests, pinned oracle), for several tile
+shapes and temporal-block depths."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from _cases import edge3d_sources, head_coeffs, load
+from conftest import rel_l2, sha
+from waveforge_b200 import (FDTD3D, Detectors, FieldSet, MurABC3D, PlaneSource, PointSource,
+                            SourceCollection, TabulatedWaveform, YeeGrid)
+
+pytestmark = pytest.mark.gpu
+
+COMPS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+TUNES3 = [None, (1, 4, 4, 4, 64), (2, 3, 5, 7, 96), (3, 6, 6, 10, 128), (1, 8, 8, 30, 256)]
+
+
+def sim3d(cuda, shape, dx, courant, srcs, ca=None, cb=None, steps=None, tune=None):
+    nx, ny, nz = shape
+    g = YeeGrid(nx, ny, dx, dx, Nz=nz, dz=dx, courant=courant, device=cuda)
+    f = FieldSet(g)
+    b = MurABC3D(g, f.Hx, f.Hy, f.Hz)
+    objs = []
+    for comp, box, wave in srcs:
+        w = TabulatedWaveform(wave)
+        i0, i1, j0, j1, k0, k1 = box
+        if (i1 - i0, j1 - j0, k1 - k0) == (1, 1, 1):
+            objs.append(PointSource(w, i0, j0, comp, k=k0, grid=g, N_steps=steps))
+        else:
+            if i1 - i0 == 1 and (j1 - j0, k1 - k0) == (ny, nz):
+                objs.append(PlaneSource(w, "yz", i0, comp, grid=g, N_steps=steps))
+            elif j1 - j0 == 1 and (i1 - i0, k1 - k0) == (nx, nz):
+                objs.append(PlaneSource(w, "xz", j0, comp, grid=g, N_steps=steps))
+            else:
+                objs.append(PlaneSource(w, "xy", k0, comp, grid=g, N_steps=steps))
+    sc = SourceCollection(objs) if objs else None
+    return FDTD3D(g, f, b, sc, Ca=None if ca is None else ca.to(cuda),
+                  Cb=None if cb is None else cb.to(cuda), n_check=10 ** 9, tune=tune), f
+
+
+def test_head3d_bit_exact_vs_reference(cuda):
+    g = load("head3d_32")
+    ca, cb = head_coeffs(g)
+    n, steps = int(g["n"]), int(g["steps"])
+    i, j, k = (int(v) for v in g["src"])
+    for tune in TUNES3:
+        sim, f = sim3d(cuda, (n, n, n), float(g["dx"]), float(g["courant"]),
+                       [("Ez", (i, i + 1, j, j + 1, k, k + 1), torch.from_numpy(g["wave"]))],
+                       ca, cb, steps=steps, tune=tune)
+        tr = sim.run(steps, record=Detectors([("Ez", *(int(v) for v in r)) for r in g["rx"]]))
+        assert sha(tr) == str(g["sha_traces"]), tune
+        for c in COMPS:
+            assert sha(getattr(f, c)) == str(g[f"sha_{c.lower()}"]), (tune, c)
+        assert rel_l2(tr.cpu().numpy(), g["traces64"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["box9x7x6", "flat8x6x1"])
+def test_edge_cases_3d_bit_exact_vs_reference(cuda, name):
+    d = load(f"edges3d_{name}")
+    shape = tuple(int(v) for v in d["shape"])
+    steps = int(d["steps"])
+    probes = [(COMPS[c], i, j, k) for c, i, j, k in d["probes"]]
+    for tune in TUNES3:
+        sim, f = sim3d(cuda, shape, 1e-3, float(d["courant"]), edge3d_sources(d), steps=steps,
+                       tune=tune)
+        tr = sim.run(steps, record=Detectors(probes))
+        for c in COMPS:
+            assert np.array_equal(getattr(f, c).cpu().numpy(), d[c.lower() + "32"]), (tune, c)
+        assert np.array_equal(tr.cpu().numpy(), d["traces32"]), tune
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_3d_bit_exact_vs_oracle(cuda, seed):
+    rng = np.random.default_rng(300 + seed)
+    shape = tuple(int(v) for v in rng.integers(4, 19, 3))
+    steps = int(rng.integers(1, 30))
+    nx, ny, nz = shape
+    srcs = []
+    for _ in range(int(rng.integers(1, 5))):
+        c = COMPS[rng.integers(0, 6)]
+        i, j, k = int(rng.integers(0, nx)), int(rng.integers(0, ny)), int(rng.integers(0, nz))
+        srcs.append((c, (i, i + 1, j, j + 1, k, k + 1),
+                     torch.from_numpy(rng.standard_normal(steps).astype(np.float32))))
+    ca = cb = None
+    if seed % 2:
+        ca = torch.from_numpy(rng.uniform(0.3, 1.0, shape).astype(np.float32))
+        cb = torch.from_numpy(rng.uniform(0.001, 0.1, shape).astype(np.float32))
+    dt = oracle.stable_dt(1e-3, 1e-3, 1e-3, 0.9)
+    o = oracle.Oracle3D(nx, ny, nz, 1e-3, 1e-3, 1e-3, dt, ca, cb)
+    for c, box, w in srcs:
+        o.add_box_source(c, box, w)
+    probes = [(COMPS[rng.integers(0, 6)], int(rng.integers(0, nx)), int(rng.integers(0, ny)),
+               int(rng.integers(0, nz))) for _ in range(6)]
+    tr_o = o.run(steps, probes)
+    for tune in TUNES3:
+        sim, f = sim3d(cuda, shape, 1e-3, 0.9, srcs, ca, cb, steps=steps, tune=tune)
+        tr = sim.run(steps, record=Detectors(probes))
+        assert np.array_equal(tr.cpu().numpy(), tr_o.numpy()), tune
+        for c in COMPS:
+            assert np.array_equal(getattr(f, c).cpu().numpy(), getattr(o, c).numpy()), (tune, c)

@@ -1,0 +1,142 @@
+"""ctypes binding of the C-ABI library ``lib/libwfb200.so`` (declared in
+``include/waveforge_b200.h``).
+
+The structures below mirror the C structs field for field; a CPU test
+compiles the header with gcc and checks sizes and offsets against them.  The
+library is loaded lazily on first use; when it is missing the product fails
+loudly (there is no CPU fallback for any compute path).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_double, c_float, c_int32, c_int64, c_void_p, POINTER
+from pathlib import Path
+from typing import Optional
+
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libwfb200.so"
+
+WF_OK, WF_E_ARG, WF_E_CUDA, WF_E_LIMIT, WF_E_DIVERGED, WF_E_TIMEOUT = range(6)
+COMP_CODE = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
+
+EXPORTED = ("wf_abi_version", "wf_last_error", "wf_fdtd2d_run", "wf_fdtd3d_run",
+            "wf_batch2d_run", "wf_das2d")
+
+
+class NativeError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[wf status {code}] {message}")
+        self.code = code
+
+
+class WfGrid2D(ctypes.Structure):
+    _fields_ = [("nx", c_int32), ("ny", c_int32), ("dh", c_float), ("de", c_float),
+                ("dx", c_float), ("dy", c_float), ("mur_x", c_float), ("mur_y", c_float)]
+
+
+class WfGrid3D(ctypes.Structure):
+    _fields_ = [("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("dh", c_float),
+                ("de", c_float), ("dx", c_float), ("dy", c_float), ("dz", c_float),
+                ("mur_x", c_float), ("mur_y", c_float), ("mur_z", c_float)]
+
+
+class WfSource(ctypes.Structure):
+    _fields_ = [("comp", c_int32), ("i0", c_int32), ("i1", c_int32), ("j0", c_int32),
+                ("j1", c_int32), ("k0", c_int32), ("k1", c_int32), ("n_wave", c_int32),
+                ("wave", c_void_p), ("amp", c_void_p)]
+
+
+class WfProbe(ctypes.Structure):
+    _fields_ = [("comp", c_int32), ("i", c_int32), ("j", c_int32), ("k", c_int32)]
+
+
+class WfTune(ctypes.Structure):
+    _fields_ = [("steps_per_pass", c_int32), ("tile_i", c_int32), ("tile_j", c_int32),
+                ("tile_k", c_int32), ("threads", c_int32)]
+
+
+class WfSolve2D(ctypes.Structure):
+    _fields_ = [("g", WfGrid2D),
+                ("ex", c_void_p), ("ey", c_void_p), ("hz", c_void_p),
+                ("sx", c_void_p), ("sy", c_void_p), ("sz", c_void_p),
+                ("ca", c_void_p), ("cb", c_void_p),
+                ("src", c_void_p), ("probes", c_void_p), ("traces", c_void_p),
+                ("trace_ld", c_int64),
+                ("nsrc", c_int32), ("nprobe", c_int32), ("trace_step0", c_int32),
+                ("step0", c_int32), ("nsteps", c_int32), ("n_check", c_int32),
+                ("status", c_int32), ("check_max", c_void_p)]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load() -> ctypes.CDLL:
+    """Load and type the library (raises RuntimeError when it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"waveforge_b200 CUDA library missing at {LIB_PATH}; build it with "
+            "`python -m waveforge_b200.csrc.build` (there is no CPU fallback)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    lib.wf_abi_version.restype = c_int32
+    lib.wf_last_error.restype = ctypes.c_char_p
+    lib.wf_fdtd2d_run.restype = c_int32
+    lib.wf_fdtd2d_run.argtypes = [
+        POINTER(WfGrid2D), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+        c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int32,
+        c_int32, c_int32, c_int32, c_void_p, POINTER(WfTune), c_void_p]
+    lib.wf_fdtd3d_run.restype = c_int32
+    lib.wf_fdtd3d_run.argtypes = [
+        POINTER(WfGrid3D), POINTER(c_void_p), POINTER(c_void_p), c_void_p, c_void_p,
+        c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int32, c_int32, c_int32,
+        c_int32, c_void_p, POINTER(WfTune), c_void_p]
+    lib.wf_batch2d_run.restype = c_int32
+    lib.wf_batch2d_run.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, POINTER(WfTune),
+                                   c_int32, c_void_p]
+    lib.wf_das2d.restype = c_int32
+    lib.wf_das2d.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
+                             c_void_p, c_int32, c_double, c_double, c_int32, c_int32, c_void_p,
+                             c_void_p]
+    if lib.wf_abi_version() != 1:
+        raise RuntimeError("waveforge_b200 CUDA library ABI mismatch; rebuild it")
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != WF_OK:
+        msg = load().wf_last_error().decode(errors="replace")
+        raise NativeError(rc, msg)
+
+
+def ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def require_cuda(t: torch.Tensor, what: str) -> None:
+    if not t.is_cuda:
+        raise RuntimeError(
+            f"{what} must live on a CUDA device: waveforge_b200 runs only on the GPU "
+            "(there is no CPU fallback)")
+
+
+def to_device_bytes(arr: ctypes.Array, device: torch.device) -> torch.Tensor:
+    """Copy a ctypes struct array into a device byte tensor (descriptor upload)."""
+    raw = bytes(memoryview(arr).cast("B"))
+    host = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
+    return host.to(device, non_blocking=False)
+
+
+def f32(x: float) -> float:
+    """Round a Python float to float32 (the scalar rounding PyTorch applies)."""
+    return float(torch.tensor(x, dtype=torch.float32).item())

@@ -1,0 +1,226 @@
+"""Batched execution of many independent, uneven 2D TM solves.
+
+The reference runs a MIMO study one ``FDTD2D`` at a time, one transmitter
+after another (examples/brain_mimo_imaging.py:149-204,
+examples/10_breast_tumor_mimo.py:123-145; on two GPUs one Python thread per
+GPU).  ``Batch2D`` places every solve's fields, scratch, coefficients,
+sources and detector traces on the device once, and advances all of them in
+ONE persistent launch of ``wf_batch2d_run``: resident CTAs pull solves from a
+device work queue in largest-first order and run each through its steps with
+the same tile routine as ``FDTD2D``, so every solve's traces are
+bit-identical to running it alone.  Solves that share a phantom share its
+``Ca``/``Cb`` tensors.
+
+``run_plain`` runs the same solves one after another through
+``wf_fdtd2d_run`` (the plain per-solve path) for comparison.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import torch
+
+from . import _native as nat
+from .core._engine import ProbeTable, SourceTable, source_list, tune_struct
+from .core.boundaries import _mur_coeff
+from .core.grid import YeeGrid
+from .detectors import Detectors
+
+EPS0: float = 8.8541878128e-12
+MU0: float = 1.2566370614e-6
+_ALLOWED = ("Ex", "Ey", "Hz")
+
+
+@dataclass
+class BatchSolve:
+    """One independent solve: grid, coefficients (None = vacuum), sources, detectors."""
+
+    grid: YeeGrid
+    sources: object
+    detectors: Optional[Detectors] = None
+    Ca: Optional[torch.Tensor] = None
+    Cb: Optional[torch.Tensor] = None
+    n_check: int = 0
+    tag: object = None
+    _state: dict = field(default_factory=dict, repr=False)
+
+
+def grid_struct(grid: YeeGrid) -> nat.WfGrid2D:
+    """Float32-rounded constants of a 2D grid, with the Mur coefficients and
+    their (-1, 0) validation of ``MurABC`` (src/core/boundaries.py:177-190)."""
+    dt = grid.dt
+    cm = [_mur_coeff(dt, grid.dx), _mur_coeff(dt, grid.dy)]
+    for ax, c in zip("xy", cm):
+        if not (-1.0 < c < 0.0):
+            raise ValueError(f"C_mur_{ax}={c!r} is not in the open interval (-1, 0). This "
+                             f"indicates a CFL violation — reduce dt or increase d{ax}.")
+    return nat.WfGrid2D(grid.Nx, grid.Ny, nat.f32(dt / MU0), nat.f32(dt / EPS0), nat.f32(grid.dx),
+                        nat.f32(grid.dy), nat.f32(cm[0]), nat.f32(cm[1]))
+
+
+class Batch2D:
+    """Device-resident set of solves advanced by one persistent launch per call."""
+
+    def __init__(self, solves: Sequence[BatchSolve], n_steps: int, *, tune=None,
+                 ctas_per_sm: int = 0, device=None) -> None:
+        if not solves:
+            raise ValueError("Batch2D needs at least one solve")
+        self.device = torch.device(device) if device is not None else solves[0].grid.device
+        if self.device.type != "cuda":
+            raise RuntimeError("Batch2D runs on a CUDA device only (no CPU fallback)")
+        nat.load()
+        self.solves = list(solves)
+        self.n_steps = n_steps
+        self.tune = tune_struct(tune)
+        self.ctas_per_sm = ctas_per_sm
+        self.step = 0
+        n = len(self.solves)
+        # one flat allocation per role keeps the descriptor upload simple
+        sizes = [s.grid.Nx * s.grid.Ny for s in self.solves]
+        offs = [0]
+        for sz in sizes:
+            offs.append(offs[-1] + sz)
+        total = offs[-1]
+        self._state = torch.zeros((3, total), dtype=torch.float32, device=self.device)
+        self._scratch = torch.empty((3, total), dtype=torch.float32, device=self.device)
+        self._offs = offs
+        nprb = [len(s.detectors) if s.detectors is not None else 0 for s in self.solves]
+        toffs = [0]
+        for q in nprb:
+            toffs.append(toffs[-1] + q * n_steps)
+        self._traces = torch.zeros(max(1, toffs[-1]), dtype=torch.float32, device=self.device)
+        self._toffs = toffs
+        self._tables = []
+        self._desc = (nat.WfSolve2D * n)()
+        for q, s in enumerate(self.solves):
+            g = s.grid
+            if g.Nx < 4 or g.Ny < 4:
+                raise ValueError(f"solve {q}: grid {g.Nx}x{g.Ny} below 4x4")
+            st = SourceTable(source_list(s.sources), self.device, _ALLOWED, 2)
+            st.check_range(0, n_steps)
+            pt = (s.detectors.table(self.device, _ALLOWED, (g.Nx, g.Ny, 1))
+                  if s.detectors is not None else None)
+            ca = None if s.Ca is None else s.Ca.to(self.device, torch.float32).contiguous()
+            cb = None if s.Cb is None else s.Cb.to(self.device, torch.float32).contiguous()
+            if (ca is None) != (cb is None):
+                raise ValueError(f"solve {q}: Ca and Cb must be given together")
+            if ca is not None and ca.numel() != g.Nx * g.Ny:
+                raise ValueError(f"solve {q}: Ca/Cb must have Nx*Ny elements")
+            self._tables.append((st, pt, ca, cb))
+            d = self._desc[q]
+            d.g = grid_struct(g)
+            o = offs[q]
+            el = 4
+            d.ex = self._state[0].data_ptr() + o * el
+            d.ey = self._state[1].data_ptr() + o * el
+            d.hz = self._state[2].data_ptr() + o * el
+            d.sx = self._scratch[0].data_ptr() + o * el
+            d.sy = self._scratch[1].data_ptr() + o * el
+            d.sz = self._scratch[2].data_ptr() + o * el
+            d.ca = nat.ptr(ca)
+            d.cb = nat.ptr(cb)
+            d.src = st.ptr
+            d.nsrc = st.count
+            d.probes = None if pt is None else pt.ptr
+            d.nprobe = 0 if pt is None else pt.count
+            d.traces = self._traces.data_ptr() + toffs[q] * el
+            d.trace_ld = n_steps
+            d.trace_step0 = 0
+            d.n_check = 0
+            d.check_max = None
+        order = sorted(range(n), key=lambda q: -sizes[q])
+        self._order = torch.tensor(order, dtype=torch.int32, device=self.device)
+        self._queue = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._desc_dev = None
+
+    # ------------------------------------------------------------------
+    @property
+    def cells(self) -> int:
+        return self._offs[-1]
+
+    def _upload(self, step0: int, nsteps: int) -> None:
+        for d in self._desc:
+            d.step0 = step0
+            d.nsteps = nsteps
+            d.status = 0
+        raw = bytes(memoryview(self._desc).cast("B"))
+        host = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
+        if self._desc_dev is None:
+            self._desc_dev = torch.empty_like(host, device=self.device)
+        self._desc_dev.copy_(host)
+
+    def run(self, nsteps: Optional[int] = None) -> None:
+        """Advance every solve ``nsteps`` (default: all remaining) in one launch."""
+        nsteps = self.n_steps - self.step if nsteps is None else nsteps
+        if nsteps <= 0:
+            return
+        if self.step + nsteps > self.n_steps:
+            raise IndexError(f"batch was built for {self.n_steps} steps")
+        self._upload(self.step, nsteps)
+        self.launch()
+        self.step += nsteps
+
+    def launch(self) -> None:
+        """Queue reset + the persistent launch (capturable in a CUDA graph)."""
+        self._queue.zero_()
+        lib = nat.load()
+        nat.check(lib.wf_batch2d_run(self._desc_dev.data_ptr(), len(self.solves),
+                                     self._order.data_ptr(), self._queue.data_ptr(),
+                                     None if self.tune is None else ctypes.byref(self.tune),
+                                     self.ctas_per_sm, nat.stream_handle(self.device)))
+
+    def statuses(self) -> list[int]:
+        raw = self._desc_dev.cpu().numpy().tobytes()
+        arr = (nat.WfSolve2D * len(self.solves)).from_buffer_copy(raw)
+        return [d.status for d in arr]
+
+    def traces(self, q: int) -> torch.Tensor:
+        """``(N_rx, n_steps)`` traces of solve q."""
+        s = self.solves[q]
+        nr = 0 if s.detectors is None else len(s.detectors)
+        return self._traces[self._toffs[q]:self._toffs[q] + nr * self.n_steps].view(nr, self.n_steps)
+
+    def traces_block(self, q0: int, n: int) -> torch.Tensor:
+        """Traces of solves q0..q0+n-1 as one ``(n, N_rx, n_steps)`` view (all
+        must record the same number of receivers; their buffers are adjacent)."""
+        nr = len(self.solves[q0].detectors)
+        for q in range(q0, q0 + n):
+            if self.solves[q].detectors is None or len(self.solves[q].detectors) != nr:
+                raise ValueError("traces_block needs solves with equal receiver counts")
+        base = self._toffs[q0]
+        return self._traces[base:base + n * nr * self.n_steps].view(n, nr, self.n_steps)
+
+    def fields(self, q: int) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        g = self.solves[q].grid
+        o0, o1 = self._offs[q], self._offs[q + 1]
+        return tuple(self._state[c, o0:o1].view(g.Nx, g.Ny, 1) for c in range(3))
+
+    def reset(self) -> None:
+        self._state.zero_()
+        self._traces.zero_()
+        self.step = 0
+
+    # ------------------------------------------------------------------
+    def run_plain_one(self, q: int, nsteps: Optional[int] = None, tune=None) -> None:
+        """Solve q alone through ``wf_fdtd2d_run`` (the plain per-solve path),
+        from step ``self.step``; does not advance ``self.step``."""
+        nsteps = self.n_steps - self.step if nsteps is None else nsteps
+        lib = nat.load()
+        d = self._desc[q]
+        st, pt, ca, cb = self._tables[q]
+        t = tune_struct(tune)
+        nat.check(lib.wf_fdtd2d_run(
+            ctypes.byref(d.g), d.ex, d.ey, d.hz, d.sx, d.sy, d.sz, d.ca, d.cb, st.ptr, st.count,
+            None if pt is None else pt.ptr, 0 if pt is None else pt.count, d.traces, d.trace_ld,
+            0, self.step, nsteps, 0, None, None if t is None else ctypes.byref(t),
+            nat.stream_handle(self.device)))
+
+    def run_plain(self, nsteps: Optional[int] = None, tune=None) -> None:
+        """The same solves, one ``wf_fdtd2d_run`` each (plain per-solve path)."""
+        nsteps = self.n_steps - self.step if nsteps is None else nsteps
+        for q in range(len(self._desc)):
+            self.run_plain_one(q, nsteps, tune)
+        self.step += nsteps

@@ -1,0 +1,194 @@
+"""Host side of the CUDA time loop shared by FDTD2D and FDTD3D.
+
+Responsibilities: translate the reference objects (sources, detectors,
+material tensors) into C-ABI descriptors once, own the ping-pong scratch
+fields, call the C-ABI for a block of steps, and turn the device-side
+stability maxima into the reference's telemetry and SimulationDivergedError
+(src/core/fdtd2d.py:268-295).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import torch
+
+from .. import _native as nat
+
+
+class SimulationDivergedError(RuntimeError):
+    """Field magnitude above the stability threshold (src/core/fdtd2d.py:48-62)."""
+
+    def __init__(self, message: str) -> None:
+        super().__init__(message)
+
+
+def source_list(sources) -> list:
+    """Flatten a SourceCollection / single injector into injector objects."""
+    if sources is None:
+        return []
+    if hasattr(sources, "sources"):
+        return list(sources.sources)
+    if hasattr(sources, "_sources"):
+        return list(sources._sources)
+    if hasattr(sources, "native_boxes"):
+        return [sources]
+    raise TypeError(f"unsupported source object {type(sources).__name__}: the CUDA engine needs "
+                    "PointSource / LineSource / PlaneSource injectors (or a SourceCollection)")
+
+
+class SourceTable:
+    """Device array of wf_source boxes plus the tensors they point at."""
+
+    def __init__(self, injectors: Sequence, device: torch.device, allowed: Sequence[str],
+                 dims: int) -> None:
+        boxes = []
+        for inj in injectors:
+            if not hasattr(inj, "native_boxes"):
+                raise TypeError(f"unsupported source {type(inj).__name__} for the CUDA engine")
+            boxes.extend(inj.native_boxes())
+        self.keep = []
+        self.n_wave_min = None
+        arr = (nat.WfSource * max(1, len(boxes)))()
+        for q, (comp, i0, i1, j0, j1, k0, k1, wave, amp) in enumerate(boxes):
+            if comp not in allowed:
+                raise KeyError(f"source component {comp!r} is not a field of the {dims}D engine "
+                               f"(allowed: {tuple(allowed)})")
+            wave = wave.contiguous()
+            if wave.dtype != torch.float32:
+                raise TypeError("source waveforms must be float32 on the CUDA engine")
+            if wave.device != device:
+                wave = wave.to(device)
+            self.keep.append(wave)
+            if amp is not None:
+                amp = amp.to(device=device, dtype=torch.float32).contiguous()
+                self.keep.append(amp)
+            arr[q] = nat.WfSource(nat.COMP_CODE[comp], i0, i1, j0, j1, k0, k1, wave.numel(),
+                                  wave.data_ptr(), None if amp is None else amp.data_ptr())
+            n = wave.numel()
+            self.n_wave_min = n if self.n_wave_min is None else min(self.n_wave_min, n)
+        self.count = len(boxes)
+        self.dev = nat.to_device_bytes(arr, device) if boxes else None
+
+    def check_range(self, step0: int, nsteps: int) -> None:
+        if self.count and step0 + nsteps > self.n_wave_min:
+            raise IndexError(f"a source waveform holds {self.n_wave_min} steps but steps up to "
+                             f"{step0 + nsteps - 1} were requested (build sources with a larger "
+                             "N_steps)")
+
+    @property
+    def ptr(self) -> Optional[int]:
+        return None if self.dev is None else self.dev.data_ptr()
+
+
+class ProbeTable:
+    """Device array of wf_probe points."""
+
+    def __init__(self, probes: Sequence[tuple], device: torch.device, allowed: Sequence[str],
+                 shape: tuple) -> None:
+        arr = (nat.WfProbe * max(1, len(probes)))()
+        for q, p in enumerate(probes):
+            comp = p[0]
+            idx = tuple(int(v) for v in p[1:]) + (0,) * (4 - len(p))
+            if comp not in allowed:
+                raise KeyError(f"probe component {comp!r} not allowed (allowed: {tuple(allowed)})")
+            for ax, (v, n) in enumerate(zip(idx, shape)):
+                if not (0 <= v < n):
+                    raise ValueError(f"probe {p} index {v} out of range [0, {n}) on axis {ax}")
+            arr[q] = nat.WfProbe(nat.COMP_CODE[comp], *idx[:3])
+        self.count = len(probes)
+        self.dev = nat.to_device_bytes(arr, device) if probes else None
+
+    @property
+    def ptr(self) -> Optional[int]:
+        return None if self.dev is None else self.dev.data_ptr()
+
+
+class EngineBase:
+    """Shared telemetry / stability bookkeeping."""
+
+    _components: tuple[str, ...] = ()
+
+    def _init_common(self, stability_threshold: float, n_check: int) -> None:
+        self._threshold = stability_threshold
+        self._n_check = n_check
+        self.steps_completed = 0
+        self.elapsed_time = 0.0
+        self.mcells_per_second = 0.0
+        self.last_field_max = -1.0
+        self.n_stability_checks = 0
+        self._src_key = None
+        self._src_table: Optional[SourceTable] = None
+
+    def _check_buffer(self, step0: int, nsteps: int):
+        nc = self._n_check
+        if nc <= 0:
+            return None, 0
+        count = (step0 + nsteps) // nc - step0 // nc
+        if count == 0:
+            return None, 0
+        buf = torch.zeros(count * len(self._components), dtype=torch.int32, device=self._device)
+        return buf, count
+
+    def _process_checks(self, buf: Optional[torch.Tensor], count: int, step0: int) -> None:
+        if buf is None:
+            return
+        vals = buf.cpu().view(torch.float32).view(count, len(self._components)).tolist()
+        first = step0 // self._n_check + 1
+        for c in range(count):
+            self.n_stability_checks += 1
+            for name, v in zip(self._components, vals[c]):
+                if v > self.last_field_max:
+                    self.last_field_max = v
+                if v > self._threshold:
+                    raise SimulationDivergedError(
+                        f"Simulation diverged at step {(first + c) * self._n_check}: {name} max = "
+                        f"{v:.3e} exceeds threshold {self._threshold:.3e}. Check CFL condition "
+                        f"(dt={self._grid.dt:.3e}) and source amplitude.")
+
+    def _sources_table(self, allowed, dims) -> SourceTable:
+        injectors = source_list(self._sources)
+        key = (id(self._sources), tuple(id(s) for s in injectors))
+        if self._src_table is None or self._src_key != key:
+            self._src_table = SourceTable(injectors, self._device, allowed, dims)
+            self._src_key = key
+        return self._src_table
+
+    def reset(self) -> None:
+        """Zero fields and telemetry (src/core/fdtd2d.py:365-378)."""
+        self._fields.zero_()
+        self.steps_completed = 0
+        self.elapsed_time = 0.0
+        self.mcells_per_second = 0.0
+        self.last_field_max = -1.0
+        self.n_stability_checks = 0
+
+    @property
+    def grid(self):
+        return self._grid
+
+    @property
+    def fields(self):
+        return self._fields
+
+    @property
+    def dt(self) -> float:
+        return self._grid.dt
+
+    @property
+    def time(self) -> float:
+        return self.steps_completed * self._grid.dt
+
+    @property
+    def throughput(self) -> float:
+        return self.mcells_per_second
+
+
+def tune_struct(tune) -> Optional[ctypes.Structure]:
+    if tune is None:
+        return None
+    if isinstance(tune, nat.WfTune):
+        return tune
+    k, ti, tj, tk, th = tune
+    return nat.WfTune(k, ti, tj, tk, th)
