@@ -51,7 +51,15 @@ typedef struct wf_grid2d {
   float de;      /* dt / EPS0 (vacuum scalar path) */
   float dx, dy;
   float mur_x, mur_y;
+  int32_t flags; /* WF_FASTDIV_* bits: set only after wf_check_fastdiv passed */
 } wf_grid2d;
+
+/* wf_grid*.flags: divisions by this spacing may use the FMA-corrected
+ * reciprocal, which wf_check_fastdiv proved identical to IEEE division for
+ * every float32 input.  Without the bit the kernels use IEEE division. */
+#define WF_FASTDIV_X 1
+#define WF_FASTDIV_Y 2
+#define WF_FASTDIV_Z 4
 
 /* 3D grid constants (src/core/fdtd3d.py:206-211, boundaries.py:429-431). */
 typedef struct wf_grid3d {
@@ -59,6 +67,7 @@ typedef struct wf_grid3d {
   float dh, de;
   float dx, dy, dz;
   float mur_x, mur_y, mur_z;
+  int32_t flags; /* WF_FASTDIV_* bits */
 } wf_grid3d;
 
 /* One soft source (src/core/sources.py: PointSource :863-887, LineSource
@@ -82,7 +91,10 @@ typedef struct wf_probe {
 } wf_probe;
 
 /* Launch shape of the temporally blocked kernels. steps_per_pass = temporal
- * block depth K; tile_i x tile_j (x tile_k) = core cells written per CTA. */
+ * block depth K.  2D: tile_i x tile_j = the on-chip REGION of one CTA
+ * (core + K-cell halo on each side); it selects one of the compiled
+ * register layouts: 48x128 (512 threads), 32x128, 32x64 (256), 8x32 (64).
+ * 3D: tile_i x tile_j x tile_k = core cells per CTA.  threads: 3D only. */
 typedef struct wf_tune {
   int32_t steps_per_pass;
   int32_t tile_i, tile_j, tile_k;
@@ -92,6 +104,12 @@ typedef struct wf_tune {
 /* Library identity and the last error message of the calling thread. */
 int32_t     wf_abi_version(void);
 const char* wf_last_error(void);
+
+/* Count the float32 inputs x (all 2^32 patterns) for which the fast
+ * division by d differs from IEEE x/d; adds the count to *mismatches
+ * (device, zeroed by the caller).  No reference counterpart: it guards the
+ * bit-exactness of the spacing divisions of src/core/fdtd2d.py:232-245. */
+int32_t wf_check_fastdiv(float d, uint32_t* mismatches, void* stream);
 
 /* Advance a 2D TM grid nsteps time steps.
  * Replaces FDTD2D.step/run (src/core/fdtd2d.py:187-359) together with
@@ -165,10 +183,15 @@ typedef struct wf_solve2d {
  * next-item counter, zeroed by the caller; order[] lists solve indices,
  * largest first) and run each through all its steps with the same tile
  * routine as wf_fdtd2d_run, so each solve's result is bit-identical to
- * running it alone.  Each solve's result lands in its ex/ey/hz. */
+ * running it alone.  Each solve's result lands in its ex/ey/hz.
+ * fastdiv != 0 runs the verified fast-division code for the whole launch:
+ * every solve must then carry both WF_FASTDIV_X|Y bits (a solve without
+ * them is not computed and gets status WF_E_ARG); fastdiv == 0 uses IEEE
+ * division for all solves. */
 int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve,
                        const int32_t* order, int32_t* queue,
-                       const wf_tune* tune, int32_t ctas_per_sm, void* stream);
+                       const wf_tune* tune, int32_t ctas_per_sm,
+                       int32_t fastdiv, void* stream);
 
 /* Delay-and-sum backprojection on the device, bit-identical to the reference
  * NumPy float64 path of examples/brain_mimo_imaging.py:211-266 (and its

@@ -111,7 +111,8 @@ class _OracleBase:
     # -- sources --------------------------------------------------------
     def add_point_source(self, comp: str, i: int, j: int, wave: torch.Tensor, k: int = 0):
         """PointSource: amplitude tensor 1.0, values = w[n:n+1]*amp (sources.py:882-887)."""
-        idx = (i, j) if self.dims == 2 else (i, j, k)
+        cell = (i, j) if self.dims == 2 else (i, j, k)
+        idx = tuple(torch.tensor([v]) for v in cell)   # index tensors, as sources.py:882-884
         self.sources.append(_Src(comp, idx, wave.to(self.dtype),
                                  torch.ones(1, dtype=self.dtype)))
 

@@ -42,8 +42,8 @@ def test_every_declared_entry_point_is_exported():
 
 
 STRUCTS = {
-    "wf_grid2d": (nat.WfGrid2D, ["nx", "ny", "dh", "de", "dx", "dy", "mur_x", "mur_y"]),
-    "wf_grid3d": (nat.WfGrid3D, ["nx", "nz", "dh", "dz", "mur_z"]),
+    "wf_grid2d": (nat.WfGrid2D, ["nx", "ny", "dh", "de", "dx", "dy", "mur_x", "mur_y", "flags"]),
+    "wf_grid3d": (nat.WfGrid3D, ["nx", "nz", "dh", "dz", "mur_z", "flags"]),
     "wf_source": (nat.WfSource, ["comp", "k1", "n_wave", "wave", "amp"]),
     "wf_probe": (nat.WfProbe, ["comp", "i", "j", "k"]),
     "wf_tune": (nat.WfTune, ["steps_per_pass", "tile_k", "threads"]),
@@ -76,7 +76,7 @@ def test_ctypes_layout_matches_c(tmp_path: Path):
 def test_argument_errors_need_no_gpu():
     """Validation happens on the host before any CUDA call."""
     lib = nat.load()
-    g = nat.WfGrid2D(3, 3, 1.0, 1.0, 1.0, 1.0, -0.5, -0.5)
+    g = nat.WfGrid2D(3, 3, 1.0, 1.0, 1.0, 1.0, -0.5, -0.5, 0)
     rc = lib.wf_fdtd2d_run(ctypes.byref(g), 1, 1, 1, 1, 1, 1, None, None, None, 0, None, 0, None,
                            0, 0, 0, 10, 0, None, None, None)
     assert rc == nat.WF_E_ARG

@@ -21,8 +21,9 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libwfb200.so"
 WF_OK, WF_E_ARG, WF_E_CUDA, WF_E_LIMIT, WF_E_DIVERGED, WF_E_TIMEOUT = range(6)
 COMP_CODE = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
 
-EXPORTED = ("wf_abi_version", "wf_last_error", "wf_fdtd2d_run", "wf_fdtd3d_run",
-            "wf_batch2d_run", "wf_das2d")
+EXPORTED = ("wf_abi_version", "wf_last_error", "wf_check_fastdiv", "wf_fdtd2d_run",
+            "wf_fdtd3d_run", "wf_batch2d_run", "wf_das2d")
+WF_FASTDIV_X, WF_FASTDIV_Y, WF_FASTDIV_Z = 1, 2, 4
 
 
 class NativeError(RuntimeError):
@@ -35,13 +36,14 @@ class NativeError(RuntimeError):
 
 class WfGrid2D(ctypes.Structure):
     _fields_ = [("nx", c_int32), ("ny", c_int32), ("dh", c_float), ("de", c_float),
-                ("dx", c_float), ("dy", c_float), ("mur_x", c_float), ("mur_y", c_float)]
+                ("dx", c_float), ("dy", c_float), ("mur_x", c_float), ("mur_y", c_float),
+                ("flags", c_int32)]
 
 
 class WfGrid3D(ctypes.Structure):
     _fields_ = [("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("dh", c_float),
                 ("de", c_float), ("dx", c_float), ("dy", c_float), ("dz", c_float),
-                ("mur_x", c_float), ("mur_y", c_float), ("mur_z", c_float)]
+                ("mur_x", c_float), ("mur_y", c_float), ("mur_z", c_float), ("flags", c_int32)]
 
 
 class WfSource(ctypes.Structure):
@@ -86,6 +88,8 @@ def load() -> ctypes.CDLL:
     lib = ctypes.CDLL(str(LIB_PATH))
     lib.wf_abi_version.restype = c_int32
     lib.wf_last_error.restype = ctypes.c_char_p
+    lib.wf_check_fastdiv.restype = c_int32
+    lib.wf_check_fastdiv.argtypes = [c_float, c_void_p, c_void_p]
     lib.wf_fdtd2d_run.restype = c_int32
     lib.wf_fdtd2d_run.argtypes = [
         POINTER(WfGrid2D), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
@@ -98,7 +102,7 @@ def load() -> ctypes.CDLL:
         c_int32, c_void_p, POINTER(WfTune), c_void_p]
     lib.wf_batch2d_run.restype = c_int32
     lib.wf_batch2d_run.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, POINTER(WfTune),
-                                   c_int32, c_void_p]
+                                   c_int32, c_int32, c_void_p]
     lib.wf_das2d.restype = c_int32
     lib.wf_das2d.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                              c_void_p, c_int32, c_double, c_double, c_int32, c_int32, c_void_p,
@@ -140,3 +144,29 @@ def to_device_bytes(arr: ctypes.Array, device: torch.device) -> torch.Tensor:
 def f32(x: float) -> float:
     """Round a Python float to float32 (the scalar rounding PyTorch applies)."""
     return float(torch.tensor(x, dtype=torch.float32).item())
+
+
+_fastdiv_ok: dict = {}
+
+
+def fastdiv_ok(d: float, device: torch.device) -> bool:
+    """True when the fast exact division by float32(d) matches IEEE division
+    for every float32 input on this device (checked once per value)."""
+    key = (f32(d), str(device))
+    if key not in _fastdiv_ok:
+        lib = load()
+        cnt = torch.zeros(1, dtype=torch.int32, device=device)
+        check(lib.wf_check_fastdiv(key[0], cnt.data_ptr(), stream_handle(device)))
+        _fastdiv_ok[key] = int(cnt.item()) == 0
+    return _fastdiv_ok[key]
+
+
+def fastdiv_flags(device: torch.device, dx: float, dy: float, dz: Optional[float] = None) -> int:
+    flags = 0
+    if fastdiv_ok(dx, device):
+        flags |= WF_FASTDIV_X
+    if fastdiv_ok(dy, device):
+        flags |= WF_FASTDIV_Y
+    if dz is not None and fastdiv_ok(dz, device):
+        flags |= WF_FASTDIV_Z
+    return flags

@@ -48,7 +48,7 @@ class BatchSolve:
     _state: dict = field(default_factory=dict, repr=False)
 
 
-def grid_struct(grid: YeeGrid) -> nat.WfGrid2D:
+def grid_struct(grid: YeeGrid, device: Optional[torch.device] = None) -> nat.WfGrid2D:
     """Float32-rounded constants of a 2D grid, with the Mur coefficients and
     their (-1, 0) validation of ``MurABC`` (src/core/boundaries.py:177-190)."""
     dt = grid.dt
@@ -57,8 +57,9 @@ def grid_struct(grid: YeeGrid) -> nat.WfGrid2D:
         if not (-1.0 < c < 0.0):
             raise ValueError(f"C_mur_{ax}={c!r} is not in the open interval (-1, 0). This "
                              f"indicates a CFL violation — reduce dt or increase d{ax}.")
+    flags = 0 if device is None else nat.fastdiv_flags(device, grid.dx, grid.dy)
     return nat.WfGrid2D(grid.Nx, grid.Ny, nat.f32(dt / MU0), nat.f32(dt / EPS0), nat.f32(grid.dx),
-                        nat.f32(grid.dy), nat.f32(cm[0]), nat.f32(cm[1]))
+                        nat.f32(grid.dy), nat.f32(cm[0]), nat.f32(cm[1]), flags)
 
 
 class Batch2D:
@@ -111,7 +112,7 @@ class Batch2D:
                 raise ValueError(f"solve {q}: Ca/Cb must have Nx*Ny elements")
             self._tables.append((st, pt, ca, cb))
             d = self._desc[q]
-            d.g = grid_struct(g)
+            d.g = grid_struct(g, self.device)
             o = offs[q]
             el = 4
             d.ex = self._state[0].data_ptr() + o * el
@@ -131,6 +132,8 @@ class Batch2D:
             d.trace_step0 = 0
             d.n_check = 0
             d.check_max = None
+        both = nat.WF_FASTDIV_X | nat.WF_FASTDIV_Y
+        self._fastdiv = all((d.g.flags & both) == both for d in self._desc)
         order = sorted(range(n), key=lambda q: -sizes[q])
         self._order = torch.tensor(order, dtype=torch.int32, device=self.device)
         self._queue = torch.zeros(1, dtype=torch.int32, device=self.device)
@@ -170,7 +173,8 @@ class Batch2D:
         nat.check(lib.wf_batch2d_run(self._desc_dev.data_ptr(), len(self.solves),
                                      self._order.data_ptr(), self._queue.data_ptr(),
                                      None if self.tune is None else ctypes.byref(self.tune),
-                                     self.ctas_per_sm, nat.stream_handle(self.device)))
+                                     self.ctas_per_sm, 1 if self._fastdiv else 0,
+                                     nat.stream_handle(self.device)))
 
     def statuses(self) -> list[int]:
         raw = self._desc_dev.cpu().numpy().tobytes()

@@ -64,7 +64,8 @@ class FDTD2D(EngineBase):
         nat.load()
         self._g = nat.WfGrid2D(grid.Nx, grid.Ny, nat.f32(self._Dh), nat.f32(self._De),
                                nat.f32(grid.dx), nat.f32(grid.dy),
-                               nat.f32(boundary.C_mur_x), nat.f32(boundary.C_mur_y))
+                               nat.f32(boundary.C_mur_x), nat.f32(boundary.C_mur_y),
+                               nat.fastdiv_flags(self._device, grid.dx, grid.dy))
         self._tune = tune_struct(tune)
         self._scratch: Optional[torch.Tensor] = None
 

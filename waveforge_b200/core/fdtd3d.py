@@ -68,7 +68,8 @@ class FDTD3D(EngineBase):
             raise TypeError("FDTD3D needs a MurABC3D boundary")
         self._g = nat.WfGrid3D(grid.Nx, grid.Ny, grid.Nz, nat.f32(self._Dh), nat.f32(self._De),
                                nat.f32(dx), nat.f32(dy), nat.f32(dz), nat.f32(boundary.C_mur_x),
-                               nat.f32(boundary.C_mur_y), nat.f32(boundary.C_mur_z))
+                               nat.f32(boundary.C_mur_y), nat.f32(boundary.C_mur_z),
+                               nat.fastdiv_flags(self._device, dx, dy, dz))
         self._tune = tune_struct(tune)
         self._scratch: Optional[torch.Tensor] = None
 

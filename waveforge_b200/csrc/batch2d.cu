@@ -11,12 +11,12 @@
 #include <algorithm>
 
 #include "tile2d.cuh"
+#include "tile2d_cfg.cuh"
 
 namespace wf {
 
-template <bool MAT>
-__device__ void run_solve(const wf_solve2d& S, int K, int ti, int tj, float* sm, Lists2D& L,
-                          int* status) {
+template <class C, bool MAT, bool FDIV>
+__device__ void run_solve(const wf_solve2d& S, int K, TileSmem<C>& sm, int* status) {
   Tile2D P{};
   P.nx = S.g.nx;
   P.ny = S.g.ny;
@@ -26,6 +26,7 @@ __device__ void run_solve(const wf_solve2d& S, int K, int ti, int tj, float* sm,
   P.dy = S.g.dy;
   P.mx = S.g.mur_x;
   P.my = S.g.mur_y;
+  P.fastdiv = S.g.flags;
   P.ca = S.ca;
   P.cb = S.cb;
   P.src = S.src;
@@ -41,7 +42,6 @@ __device__ void run_solve(const wf_solve2d& S, int K, int ti, int tj, float* sm,
   P.status = status;
   float* A[3] = {S.ex, S.ey, S.hz};
   float* B[3] = {S.sx, S.sy, S.sz};
-  const int tiles_i = (P.nx + ti - 1) / ti, tiles_j = (P.ny + tj - 1) / tj;
   const PassPlan plan(S.nsteps, K);
   for (int p = 0; p < plan.passes(); ++p) {
     float** in = (p & 1) ? B : A;
@@ -53,18 +53,16 @@ __device__ void run_solve(const wf_solve2d& S, int K, int ti, int tj, float* sm,
     P.ey_out = out[1];
     P.hz_out = out[2];
     const int s0 = S.step0 + plan.offset(p), k = plan.len(p);
-    for (int bi = 0; bi < tiles_i; ++bi)
-      for (int bj = 0; bj < tiles_j; ++bj) {
-        const int ci0 = bi * ti, cj0 = bj * tj;
-        tile2d<MAT>(P, ci0, min(ci0 + ti, P.nx), cj0, min(cj0 + tj, P.ny), s0, k, sm, L);
-      }
-    // tile2d ends with a CTA barrier; global writes of this pass are visible
-    // to every thread of the CTA before the next pass reads them.
-    __threadfence_block();
+    const int ci = C::RH - 2 * k, cj = C::RW - 2 * k;
+    for (int ci0 = 0; ci0 < P.nx; ci0 += ci)
+      for (int cj0 = 0; cj0 < P.ny; cj0 += cj)
+        tile2d<C, MAT, FDIV>(P, ci0, min(ci0 + ci, P.nx), cj0, min(cj0 + cj, P.ny), s0, k, sm);
+    // tile2d ends with a CTA barrier, so this pass's global writes are
+    // visible to every thread of the CTA before the next pass reads them.
   }
   if (plan.needs_copy()) {
     const long long n = (long long)P.nx * P.ny;
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+    for (long long i = threadIdx.x; i < n; i += C::THREADS) {
       S.ex[i] = S.sx[i];
       S.ey[i] = S.sy[i];
       S.hz[i] = S.sz[i];
@@ -73,11 +71,12 @@ __device__ void run_solve(const wf_solve2d& S, int K, int ti, int tj, float* sm,
   }
 }
 
-__global__ void __launch_bounds__(512, 1) k_batch2d(const wf_solve2d* __restrict__ solves,
-                                                  const int* __restrict__ order, int nsolve,
-                                                  int* queue, int K, int ti, int tj) {
-  extern __shared__ float sm[];
-  __shared__ Lists2D L;
+template <class C, bool FDIV>
+__global__ void __launch_bounds__(C::THREADS, 1) k_batch2d(const wf_solve2d* __restrict__ solves,
+                                                           const int* __restrict__ order,
+                                                           int nsolve, int* queue, int K) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TileSmem<C>& sm = *reinterpret_cast<TileSmem<C>*>(smraw);
   __shared__ int s_item;
   __shared__ int s_status;
   for (;;) {
@@ -88,20 +87,52 @@ __global__ void __launch_bounds__(512, 1) k_batch2d(const wf_solve2d* __restrict
     __syncthreads();
     const int it = s_item;
     if (it >= nsolve) return;
-    const int si = order[it];
-    const wf_solve2d& S = solves[si];
-    if (S.nsteps > 0) {
-      if (S.ca != nullptr) run_solve<true>(S, K, ti, tj, sm, L, &s_status);
-      else run_solve<false>(S, K, ti, tj, sm, L, &s_status);
+    const wf_solve2d& S = solves[order[it]];
+    const bool flagged = (S.g.flags & (WF_FASTDIV_X | WF_FASTDIV_Y)) == (WF_FASTDIV_X | WF_FASTDIV_Y);
+    if (FDIV && !flagged) {
+      // a launch in fast-division mode only runs solves whose spacings passed
+      // wf_check_fastdiv; anything else is reported, not computed
+      if (threadIdx.x == 0) s_status = WF_E_ARG;
+    } else if (S.nsteps > 0) {
+      if (S.ca != nullptr) run_solve<C, true, FDIV>(S, K, sm, &s_status);
+      else run_solve<C, false, FDIV>(S, K, sm, &s_status);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      // Overwrite the solve's status word (it is only written by its owner).
-      const_cast<wf_solve2d&>(S).status = s_status;
-    }
+    if (threadIdx.x == 0) const_cast<wf_solve2d&>(S).status = s_status;
     __syncthreads();
   }
 }
+
+struct LaunchBatch {
+  const wf_solve2d* solves;
+  const int* order;
+  int nsolve;
+  int* queue;
+  int K, ctas_per_sm, nsm;
+  bool fdiv;
+  cudaStream_t st;
+  template <class C>
+  int operator()() const {
+    return fdiv ? go<C, true>() : go<C, false>();
+  }
+  template <class C, bool FDIV>
+  int go() const {
+    const size_t smem = sizeof(TileSmem<C>);
+    cudaError_t e = cudaFuncSetAttribute(k_batch2d<C, FDIV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_batch2d)");
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2d<C, FDIV>, C::THREADS, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) return set_error(WF_E_LIMIT, "wf_batch2d_run: layout does not fit on an SM");
+    if (ctas_per_sm > 0) per_sm = std::min(per_sm, ctas_per_sm);
+    const int grid = std::min(nsm * per_sm, nsolve);
+    k_batch2d<C, FDIV><<<grid, C::THREADS, smem, st>>>(solves, order, nsolve, queue, K);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "launch k_batch2d");
+    return WF_OK;
+  }
+};
 
 }  // namespace wf
 
@@ -109,7 +140,7 @@ using namespace wf;
 
 extern "C" int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve, const int32_t* order,
                                   int32_t* queue, const wf_tune* tune, int32_t ctas_per_sm,
-                                  void* stream) {
+                                  int32_t fastdiv, void* stream) {
   if (nsolve < 0 || (nsolve > 0 && (solves == nullptr || order == nullptr || queue == nullptr)))
     return set_error(WF_E_ARG, "wf_batch2d_run: null descriptor/order/queue pointer");
   if (nsolve == 0) return WF_OK;
@@ -117,37 +148,16 @@ extern "C" int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve, cons
   if (tune) {
     t = *tune;
   } else {
-    t.steps_per_pass = 4;
-    t.tile_i = 24;
-    t.tile_j = 56;
-    t.threads = 256;
-    t.tile_k = 1;
+    t.steps_per_pass = 6;
+    t.tile_i = 48;
+    t.tile_j = 128;
   }
-  if (t.steps_per_pass < 1 || t.steps_per_pass > 64 || t.tile_i < 2 || t.tile_j < 2 ||
-      t.threads < 32 || t.threads > 512 || (t.threads & 31))
-    return set_error(WF_E_ARG, "wf_batch2d_run: bad tune k=%d tile=%dx%d threads=%d",
-                     t.steps_per_pass, t.tile_i, t.tile_j, t.threads);
+  if (int rc = check_tune2d(t)) return rc;
   int dev = 0, nsm = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
-  // The region of any tile is at most (tile + 2k) per side; always size for
-  // the material path so one launch serves every solve.
-  const size_t smem =
-      tile2d_smem(t.tile_i + 2 * t.steps_per_pass, t.tile_j + 2 * t.steps_per_pass, true);
-  e = cudaFuncSetAttribute(k_batch2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_batch2d)");
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch2d, t.threads, smem);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-  if (per_sm < 1)
-    return set_error(WF_E_LIMIT, "wf_batch2d_run: tune does not fit on an SM (smem %zu B)", smem);
-  if (ctas_per_sm > 0) per_sm = std::min(per_sm, (int)ctas_per_sm);
-  const int grid = std::min(nsm * per_sm, (int)nsolve);
-  k_batch2d<<<grid, t.threads, smem, (cudaStream_t)stream>>>(solves, order, nsolve, queue,
-                                                              t.steps_per_pass, t.tile_i, t.tile_j);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "launch k_batch2d");
-  return WF_OK;
+  return dispatch_cfg2d(t, LaunchBatch{solves, order, nsolve, queue, t.steps_per_pass,
+                                       ctas_per_sm, nsm, fastdiv != 0, (cudaStream_t)stream});
 }

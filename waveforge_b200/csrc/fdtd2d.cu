@@ -9,18 +9,18 @@
 #include <algorithm>
 
 #include "tile2d.cuh"
+#include "tile2d_cfg.cuh"
 
 namespace wf {
 
-template <bool MAT>
-__global__ void __launch_bounds__(512, 1) k2d_pass(Tile2D P, int ti, int tj, int tiles_j,
-                                                 int step0, int k) {
-  extern __shared__ float sm[];
-  __shared__ Lists2D L;
+template <class C, bool MAT, bool FDIV>
+__global__ void __launch_bounds__(C::THREADS, 1) k2d_pass(Tile2D P, int ci, int cj, int tiles_j,
+                                                          int step0, int k) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TileSmem<C>& S = *reinterpret_cast<TileSmem<C>*>(smraw);
   const int bi = blockIdx.x / tiles_j, bj = blockIdx.x - bi * tiles_j;
-  const int ci0 = bi * ti, cj0 = bj * tj;
-  const int ci1 = min(ci0 + ti, P.nx), cj1 = min(cj0 + tj, P.ny);
-  tile2d<MAT>(P, ci0, ci1, cj0, cj1, step0, k, sm, L);
+  const int ci0 = bi * ci, cj0 = bj * cj;
+  tile2d<C, MAT, FDIV>(P, ci0, min(ci0 + ci, P.nx), cj0, min(cj0 + cj, P.ny), step0, k, S);
 }
 
 __global__ void k_copy3(const float* __restrict__ a, const float* __restrict__ b,
@@ -37,42 +37,52 @@ __global__ void k_copy3(const float* __restrict__ a, const float* __restrict__ b
 wf_tune default_tune2d(int nx, int ny) {
   wf_tune t{};
   if ((long long)nx * ny >= 1024LL * 1024) {
-    t.steps_per_pass = 4;
-    t.tile_i = 24;
-    t.tile_j = 120;
-    t.threads = 512;
+    t.steps_per_pass = 6;
+    t.tile_i = 48;
+    t.tile_j = 128;
   } else {
     t.steps_per_pass = 4;
-    t.tile_i = 24;
-    t.tile_j = 56;
-    t.threads = 256;
+    t.tile_i = 32;
+    t.tile_j = 64;
   }
   t.tile_k = 1;
+  t.threads = 0;
   return t;
 }
 
-int validate_tune2d(const wf_tune& t) {
-  if (t.steps_per_pass < 1 || t.steps_per_pass > 64 || t.tile_i < 2 || t.tile_j < 2 ||
-      t.threads < 32 || t.threads > 512 || (t.threads & 31))
-    return set_error(WF_E_ARG, "bad 2D tune: k=%d tile=%dx%d threads=%d", t.steps_per_pass,
-                     t.tile_i, t.tile_j, t.threads);
-  return WF_OK;
-}
-
-template <bool MAT>
-static int launch_pass(const Tile2D& P, const wf_tune& t, int step0, int k, cudaStream_t st) {
-  const int tiles_i = (P.nx + t.tile_i - 1) / t.tile_i;
-  const int tiles_j = (P.ny + t.tile_j - 1) / t.tile_j;
-  const int rh = std::min(t.tile_i + 2 * k, P.nx), rw = std::min(t.tile_j + 2 * k, P.ny);
-  const size_t smem = tile2d_smem(rh, rw, MAT);
-  cudaError_t e = cudaFuncSetAttribute(k2d_pass<MAT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k2d_pass)");
-  k2d_pass<MAT><<<tiles_i * tiles_j, t.threads, smem, st>>>(P, t.tile_i, t.tile_j, tiles_j, step0, k);
-  e = cudaGetLastError();
+template <class C, bool MAT, bool FDIV>
+static int launch_pass_cfg(const Tile2D& P, int k, int step0, cudaStream_t st) {
+  const int ci = C::RH - 2 * k, cj = C::RW - 2 * k;
+  const int tiles_i = (P.nx + ci - 1) / ci, tiles_j = (P.ny + cj - 1) / cj;
+  const size_t smem = sizeof(TileSmem<C>);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k2d_pass<C, MAT, FDIV>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k2d_pass)");
+    attr_done = true;
+  }
+  const long long nblk = (long long)tiles_i * tiles_j;
+  if (nblk > 0x7fffffffLL) return set_error(WF_E_LIMIT, "wf_fdtd2d_run: too many tiles");
+  k2d_pass<C, MAT, FDIV><<<(unsigned)nblk, C::THREADS, smem, st>>>(P, ci, cj, tiles_j, step0, k);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "launch k2d_pass");
   return WF_OK;
 }
+
+struct LaunchPass {
+  const Tile2D& P;
+  int k, step0;
+  cudaStream_t st;
+  bool mat, fdiv;
+  template <class C>
+  int operator()() const {
+    if (mat) return fdiv ? launch_pass_cfg<C, true, true>(P, k, step0, st)
+                         : launch_pass_cfg<C, true, false>(P, k, step0, st);
+    return fdiv ? launch_pass_cfg<C, false, true>(P, k, step0, st)
+                : launch_pass_cfg<C, false, false>(P, k, step0, st);
+  }
+};
 
 }  // namespace wf
 
@@ -100,7 +110,7 @@ extern "C" int32_t wf_fdtd2d_run(const wf_grid2d* g, float* ex, float* ey, float
     return set_error(WF_E_LIMIT, "wf_fdtd2d_run: at most 32767 sources and probes");
   if (nsteps == 0) return WF_OK;
   const wf_tune t = tune ? *tune : default_tune2d(g->nx, g->ny);
-  if (int rc = validate_tune2d(t)) return rc;
+  if (int rc = check_tune2d(t)) return rc;
   cudaStream_t st = (cudaStream_t)stream;
 
   Tile2D P{};
@@ -112,6 +122,7 @@ extern "C" int32_t wf_fdtd2d_run(const wf_grid2d* g, float* ex, float* ey, float
   P.dy = g->dy;
   P.mx = g->mur_x;
   P.my = g->mur_y;
+  P.fastdiv = g->flags;
   P.ca = ca;
   P.cb = cb;
   P.src = src;
@@ -125,6 +136,7 @@ extern "C" int32_t wf_fdtd2d_run(const wf_grid2d* g, float* ex, float* ey, float
   P.check_max = check_max;
   P.check_base = n_check > 0 ? step0 / n_check : 0;
   P.status = nullptr;
+  const bool fdiv = (g->flags & (WF_FASTDIV_X | WF_FASTDIV_Y)) == (WF_FASTDIV_X | WF_FASTDIV_Y);
 
   float* A[3] = {ex, ey, hz};
   float* B[3] = {sx, sy, sz};
@@ -139,7 +151,7 @@ extern "C" int32_t wf_fdtd2d_run(const wf_grid2d* g, float* ex, float* ey, float
     P.ey_out = out[1];
     P.hz_out = out[2];
     const int s0 = step0 + plan.offset(p), k = plan.len(p);
-    const int rc = ca ? launch_pass<true>(P, t, s0, k, st) : launch_pass<false>(P, t, s0, k, st);
+    const int rc = dispatch_cfg2d(t, LaunchPass{P, k, s0, st, ca != nullptr, fdiv});
     if (rc) return rc;
   }
   if (plan.needs_copy()) {

@@ -56,7 +56,12 @@ __device__ __forceinline__ float src3_value(const wf_source& s, int i, int j, in
   return fmul(w, s.amp[c]);
 }
 
-template <bool MAT>
+template <bool FDIV>
+__device__ __forceinline__ float dv(float a, float d, double r) {
+  return FDIV ? div_fast(a, r) : fdiv(a, d);
+}
+
+template <bool MAT, bool FDIV>
 __global__ void __launch_bounds__(512, 1) k3d_pass(Tile3D P, int ti, int tj, int tk, int tiles_j,
                                                 int tiles_k, int step0, int kst) {
   extern __shared__ float sm[];
@@ -81,6 +86,8 @@ __global__ void __launch_bounds__(512, 1) k3d_pass(Tile3D P, int ti, int tj, int
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const float dh = P.dh, de = P.de, dx = P.dx, dy = P.dy, dz = P.dz;
   const float mx = P.mx, my = P.my, mz = P.mz;
+  const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy),
+               rdz = __drcp_rn((double)dz);
 
   if (tid == 0) {
     int nh = 0, ne = 0;
@@ -167,18 +174,18 @@ __global__ void __launch_bounds__(512, 1) k3d_pass(Tile3D P, int ti, int tj, int
           }
         }
         if (gj < ny - 1 && gk < nz - 1 && s + 1 < RJ && u + 1 < RK) {
-          const float t1 = fdiv(fsub(E[1][o + 1], E[1][o]), dz);
-          const float t2 = fdiv(fsub(E[2][o + SJ], E[2][o]), dy);
+          const float t1 = dv<FDIV>(fsub(E[1][o + 1], E[1][o]), dz, rdz);
+          const float t2 = dv<FDIV>(fsub(E[2][o + SJ], E[2][o]), dy, rdy);
           vx = fadd(vx, fmul(dh, fsub(t1, t2)));
         }
         if (gi < nx - 1 && gk < nz - 1 && r + 1 < RI && u + 1 < RK) {
-          const float t1 = fdiv(fsub(E[2][o + SI], E[2][o]), dx);
-          const float t2 = fdiv(fsub(E[0][o + 1], E[0][o]), dz);
+          const float t1 = dv<FDIV>(fsub(E[2][o + SI], E[2][o]), dx, rdx);
+          const float t2 = dv<FDIV>(fsub(E[0][o + 1], E[0][o]), dz, rdz);
           vy = fadd(vy, fmul(dh, fsub(t1, t2)));
         }
         if (gi < nx - 1 && gj < ny - 1 && r + 1 < RI && s + 1 < RJ) {
-          const float t1 = fdiv(fsub(E[0][o + SJ], E[0][o]), dy);
-          const float t2 = fdiv(fsub(E[1][o + SI], E[1][o]), dx);
+          const float t1 = dv<FDIV>(fsub(E[0][o + SJ], E[0][o]), dy, rdy);
+          const float t2 = dv<FDIV>(fsub(E[1][o + SI], E[1][o]), dx, rdx);
           vz = fadd(vz, fmul(dh, fsub(t1, t2)));
         }
         Hb[0][o] = vx;
@@ -269,18 +276,18 @@ __global__ void __launch_bounds__(512, 1) k3d_pass(Tile3D P, int ti, int tj, int
         const int gk = rk0 + u;
         const int o = row * RK + u;
         if (gj >= 1 && gk >= 1 && s >= 1 && u >= 1) {
-          const float c = fsub(fdiv(fsub(Hb[2][o], Hb[2][o - SJ]), dy),
-                               fdiv(fsub(Hb[1][o], Hb[1][o - 1]), dz));
+          const float c = fsub(dv<FDIV>(fsub(Hb[2][o], Hb[2][o - SJ]), dy, rdy),
+                               dv<FDIV>(fsub(Hb[1][o], Hb[1][o - 1]), dz, rdz));
           E[0][o] = MAT ? fadd(fmul(ca[o], E[0][o]), fmul(cb[o], c)) : fadd(E[0][o], fmul(de, c));
         }
         if (gi >= 1 && gk >= 1 && r >= 1 && u >= 1) {
-          const float c = fsub(fdiv(fsub(Hb[0][o], Hb[0][o - 1]), dz),
-                               fdiv(fsub(Hb[2][o], Hb[2][o - SI]), dx));
+          const float c = fsub(dv<FDIV>(fsub(Hb[0][o], Hb[0][o - 1]), dz, rdz),
+                               dv<FDIV>(fsub(Hb[2][o], Hb[2][o - SI]), dx, rdx));
           E[1][o] = MAT ? fadd(fmul(ca[o], E[1][o]), fmul(cb[o], c)) : fadd(E[1][o], fmul(de, c));
         }
         if (gi >= 1 && gj >= 1 && r >= 1 && s >= 1) {
-          const float c = fsub(fdiv(fsub(Hb[1][o], Hb[1][o - SI]), dx),
-                               fdiv(fsub(Hb[0][o], Hb[0][o - SJ]), dy));
+          const float c = fsub(dv<FDIV>(fsub(Hb[1][o], Hb[1][o - SI]), dx, rdx),
+                               dv<FDIV>(fsub(Hb[0][o], Hb[0][o - SJ]), dy, rdy));
           E[2][o] = MAT ? fadd(fmul(ca[o], E[2][o]), fmul(cb[o], c)) : fadd(E[2][o], fmul(de, c));
         }
       }
@@ -349,7 +356,7 @@ __global__ void k_copy6(Tile3D P, long long n) {
     for (int c = 0; c < 6; ++c) P.out[c][i] = P.in[c][i];
 }
 
-template <bool MAT>
+template <bool MAT, bool FDIV>
 static int launch3(const Tile3D& P, const wf_tune& t, int s0, int k, cudaStream_t st) {
   const int ti = t.tile_i, tj = t.tile_j, tk = t.tile_k;
   const int tiles_i = (P.nx + ti - 1) / ti, tiles_j = (P.ny + tj - 1) / tj,
@@ -357,11 +364,11 @@ static int launch3(const Tile3D& P, const wf_tune& t, int s0, int k, cudaStream_
   const size_t smem = tile3d_smem(std::min(ti + 2 * k, P.nx), std::min(tj + 2 * k, P.ny),
                                   std::min(tk + 2 * k, P.nz), MAT);
   cudaError_t e =
-      cudaFuncSetAttribute(k3d_pass<MAT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaFuncSetAttribute(k3d_pass<MAT, FDIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k3d_pass)");
   const long long nblk = (long long)tiles_i * tiles_j * tiles_k;
   if (nblk > 0x7fffffffLL) return set_error(WF_E_LIMIT, "wf_fdtd3d_run: too many tiles");
-  k3d_pass<MAT><<<(unsigned)nblk, t.threads, smem, st>>>(P, ti, tj, tk, tiles_j, tiles_k, s0, k);
+  k3d_pass<MAT, FDIV><<<(unsigned)nblk, t.threads, smem, st>>>(P, ti, tj, tk, tiles_j, tiles_k, s0, k);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "launch k3d_pass");
   return WF_OK;
@@ -431,6 +438,9 @@ extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* con
   P.n_check = n_check;
   P.check_max = check_max;
   P.check_base = n_check > 0 ? step0 / n_check : 0;
+  const int all3 = WF_FASTDIV_X | WF_FASTDIV_Y | WF_FASTDIV_Z;
+  const int all2 = WF_FASTDIV_X | WF_FASTDIV_Y;
+  const bool fd = g->nz > 1 ? (g->flags & all3) == all3 : (g->flags & all2) == all2;
   const PassPlan plan(nsteps, t.steps_per_pass);
   for (int p = 0; p < plan.passes(); ++p) {
     float* const* in = (p & 1) ? s : f;
@@ -440,7 +450,8 @@ extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* con
       P.out[c] = out[c];
     }
     const int s0 = step0 + plan.offset(p), k = plan.len(p);
-    const int rc = ca ? launch3<true>(P, t, s0, k, st) : launch3<false>(P, t, s0, k, st);
+    const int rc = ca ? (fd ? launch3<true, true>(P, t, s0, k, st) : launch3<true, false>(P, t, s0, k, st))
+                      : (fd ? launch3<false, true>(P, t, s0, k, st) : launch3<false, false>(P, t, s0, k, st));
     if (rc) return rc;
   }
   if (plan.needs_copy()) {

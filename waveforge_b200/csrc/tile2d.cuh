@@ -1,25 +1,34 @@
 // tile2d.cuh -- the 2D TM Yee tile routine shared by the plain and batched kernels.
 //
-// One CTA advances one rectangular tile of one solve by k time steps inside
-// shared memory (overlapped temporal blocking): it loads the tile core plus a
-// k-cell halo of Ex, Ey, Hz (and Ca, Cb) from the pass-input buffers, runs k
-// complete leapfrog steps on that region, and stores the core to the
-// pass-output buffers.  The valid region shrinks by one cell per step on every
-// side that is not a domain edge, so after k steps the core is exact.
+// One CTA advances one tile of one solve by k time steps (overlapped temporal
+// blocking): it loads a region = core + k-cell halo of Ex, Ey, Hz (and Ca,
+// Cb) from the pass-input buffers, runs k complete leapfrog steps on it, and
+// stores the core to the pass-output buffers.  The valid part of the region
+// shrinks by one cell per step on every side that is not a domain edge, so
+// after k steps the core is exact.
+//
+// Register-resident layout: the region is RH x RW cells (RH = R*WY rows,
+// RW = 32*WX columns).  Warp (wx, wy) owns columns wx*32..wx*32+31 (one per
+// lane, so every global access is a coalesced 128-byte row segment) and rows
+// wy*R..wy*R+R-1; each thread keeps its R cells of Ex, Ey, Hz, Ca, Cb in
+// registers for the whole pass.  Horizontal neighbours come from warp
+// shuffles, and only the cells on warp boundaries go through small shared
+// exchange rows: two CTA barriers per step.  Tiles whose region touches no
+// domain edge run a specialisation without any boundary logic.
 //
 // Per step, in reference order (src/core/fdtd2d.py:187-266):
-//   1. soft injection into Ex/Ey (src/core/sources.py:863-887); Hz injection is
-//      folded into phase 2 so the Mur snapshot stays pre-injection
-//      (boundaries.py:237 snapshot happens before sources.step);
+//   1. soft injection into Ex/Ey (src/core/sources.py:863-887); Hz injection
+//      is folded into 2 so the Mur snapshot stays pre-injection
+//      (boundaries.py:237 snapshots before sources.step);
 //   2. Faraday update of Hz on i<Nx-1, j<Ny-1 (fdtd2d.py:232-235);
-//   3. first-order Mur on the four Hz edges, x edges then y edges, evaluated as
-//      a pure function of the pre-step Hz and the curl-updated Hz
-//      (boundaries.py:259-274);
+//   3. first-order Mur on the four Hz edges, x edges then y edges, as a pure
+//      function of the pre-step and the curl-updated Hz (boundaries.py:
+//      259-274), staged in shared memory by edge tiles only;
 //   4. Ampere updates of Ex (j>=1) and Ey (i>=1), scalar or Ca/Cb path
 //      (fdtd2d.py:244-257);
-//   5. detector gather and (every n_check steps) the |field| maxima.
-// Hz is double-buffered in shared memory (ha = previous step, hb = new), which
-// also provides the Mur snapshot for free.
+//   5. detector samples and, every n_check steps, the |field| maxima.
+// Every float op is a separately rounded IEEE op in the reference order; the
+// spacing divisions use the verified exact division of wf_common.cuh.
 #pragma once
 
 #include "wf_common.cuh"
@@ -32,6 +41,7 @@ constexpr int kMaxLocalProbe = 256;
 struct Tile2D {
   int nx, ny;
   float dh, de, dx, dy, mx, my;
+  int fastdiv;  // WF_FASTDIV_* bits of the grid
   const float *ex_in, *ey_in, *hz_in;
   float *ex_out, *ey_out, *hz_out;
   const float *ca, *cb;
@@ -48,7 +58,23 @@ struct Tile2D {
   int* status;     // device status word (may be null)
 };
 
-struct Lists2D {
+// Region geometry of one launch configuration.
+template <int R_, int WX_, int WY_>
+struct TileCfg {
+  static constexpr int R = R_, WX = WX_, WY = WY_;
+  static constexpr int THREADS = 32 * WX * WY;
+  static constexpr int RH = R * WY, RW = 32 * WX;
+};
+
+// Shared memory of the tile routine (sized for the configuration).
+template <class C>
+struct TileSmem {
+  float xe[C::RH][C::WX];   // Ex of each warp column's lane 0 (for lane 31 of the left warp)
+  float yr[C::WY][C::RW];   // Ey of each segment's first row (for the segment above)
+  float hx[C::RH][C::WX];   // Hz of each warp column's lane 31 (for lane 0 of the right warp)
+  float hr[C::WY][C::RW];   // Hz of each segment's last row (for the segment below)
+  float sp[C::RH][C::RW];   // Mur staging: pre-step Hz
+  float sc[C::RH][C::RW];   // Mur staging: curl-updated Hz
   int nh, ne, np;
   short h[kMaxLocalSrc];
   short e[kMaxLocalSrc];
@@ -64,229 +90,328 @@ __device__ __forceinline__ float src_value(const wf_source& s, int i, int j, int
   return fmul(w, s.amp[c]);
 }
 
-__device__ __forceinline__ bool src_hits(const wf_source& s, int i, int j) {
-  return i >= s.i0 && i < s.i1 && j >= s.j0 && j < s.j1;
-}
+// Per-thread view of one tile: geometry and lists fixed for the pass.
+struct TileCtx {
+  int ri0, ri1, rj0, rj1, RHa, RWa;
+  int ci0, ci1, cj0, cj1;
+  int lane, wx, wy, c, r0, gj;
+  int nh, ne, np;
+  bool my_h, my_e, pslow;
+  int pown0, pown1, pq0, pq1;
+};
 
-// Smem bytes needed for a region of rh x rw cells.
-__host__ __device__ inline size_t tile2d_smem(int rh, int rw, bool mat) {
-  return (size_t)rh * rw * (mat ? 6 : 4) * sizeof(float);
-}
-
-template <bool MAT>
-__device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1,
-                       int step0, int k, float* sm, Lists2D& L) {
+template <class C, bool MAT, bool FDIV, bool EDGE>
+__device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, TileSmem<C>& S,
+                                             float (&ex)[C::R], float (&ey)[C::R],
+                                             float (&hz)[C::R], const float (&ca)[C::R],
+                                             const float (&cb)[C::R], int step0, int k) {
+  constexpr int R = C::R, WX = C::WX, WY = C::WY;
   const int nx = P.nx, ny = P.ny;
-  const int ri0 = max(ci0 - k, 0), ri1 = min(ci1 + k, nx);
-  const int rj0 = max(cj0 - k, 0), rj1 = min(cj1 + k, ny);
-  const int RH = ri1 - ri0, RW = rj1 - rj0, RN = RH * RW;
-  float* ex = sm;
-  float* ey = ex + RN;
-  float* ha = ey + RN;
-  float* hb = ha + RN;
-  float* ca = hb + RN;
-  float* cb = ca + RN;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int lane = T.lane, wx = T.wx, wy = T.wy, c = T.c, r0 = T.r0, gj = T.gj, ri0 = T.ri0;
   const float dh = P.dh, de = P.de, dx = P.dx, dy = P.dy, mx = P.mx, my = P.my;
-
-  // ---- local source / probe lists (sources keep collection order) --------
-  if (tid == 0) {
-    int nh = 0, ne = 0;
-    for (int s = 0; s < P.nsrc; ++s) {
-      const wf_source& S = P.src[s];
-      if (S.i1 <= ri0 || S.i0 >= ri1 || S.j1 <= rj0 || S.j0 >= rj1) continue;
-      if (S.comp == WF_HZ) {
-        if (nh < kMaxLocalSrc) L.h[nh++] = (short)s;
-        else if (P.status) atomicExch(P.status, WF_E_LIMIT);
-      } else {
-        if (ne < kMaxLocalSrc) L.e[ne++] = (short)s;
-        else if (P.status) atomicExch(P.status, WF_E_LIMIT);
-      }
-    }
-    L.nh = nh;
-    L.ne = ne;
-    L.np = 0;
-    L.bmax[0] = L.bmax[1] = L.bmax[2] = 0u;
-  }
-  __syncthreads();
-  for (int q = tid; q < P.nprb; q += blockDim.x) {
-    const wf_probe& pr = P.prb[q];
-    if (pr.i >= ci0 && pr.i < ci1 && pr.j >= cj0 && pr.j < cj1) {
-      const int slot = atomicAdd(&L.np, 1);
-      if (slot < kMaxLocalProbe) L.p[slot] = (short)q;
-      else if (P.status) atomicExch(P.status, WF_E_LIMIT);
-    }
-  }
-
-  // ---- load region ---------------------------------------------------------
-  for (int r = warp; r < RH; r += nw) {
-    const long long g = (long long)(ri0 + r) * ny + rj0;
-    for (int c = lane; c < RW; c += 32) {
-      const int o = r * RW + c;
-      ex[o] = P.ex_in[g + c];
-      ey[o] = P.ey_in[g + c];
-      ha[o] = P.hz_in[g + c];
-      if (MAT) {
-        ca[o] = P.ca[g + c];
-        cb[o] = P.cb[g + c];
-      }
-    }
-  }
-  __syncthreads();
-  const int np = min(L.np, kMaxLocalProbe);
-  const int nh = L.nh, ne = L.ne;
+  const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy);
+  auto divx = [&](float a) { return FDIV ? div_fast(a, rdx) : fdiv(a, dx); };
+  auto divy = [&](float a) { return FDIV ? div_fast(a, rdy) : fdiv(a, dy); };
+  // Boundary predicates (compile away for interior tiles).
+  const bool colv = T.c < T.RWa;
+  const bool curl_col = EDGE ? (gj < ny - 1) : true;
+  const bool ex_col = EDGE ? (gj >= 1) : true;
 
   for (int t = 0; t < k; ++t) {
     const int n = step0 + t;
 
-    // (1) E-field soft injection, sequential to keep source order exact.
-    if (ne > 0) {
-      if (tid == 0) {
-        for (int q = 0; q < ne; ++q) {
-          const wf_source& S = P.src[L.e[q]];
-          float* f = (S.comp == WF_EX) ? ex : ey;
-          const int a0 = max(S.i0, ri0), a1 = min(S.i1, ri1);
-          const int b0 = max(S.j0, rj0), b1 = min(S.j1, rj1);
-          for (int i = a0; i < a1; ++i)
-            for (int j = b0; j < b1; ++j) {
-              const int o = (i - ri0) * RW + (j - rj0);
-              f[o] = fadd(f[o], src_value(S, i, j, n));
-            }
-        }
-      }
-      __syncthreads();
-    }
-
-    // (2) Hz injection + Faraday curl into hb.
-    for (int r = warp; r < RH; r += nw) {
-      const int gi = ri0 + r;
-      for (int c = lane; c < RW; c += 32) {
-        const int gj = rj0 + c;
-        const int o = r * RW + c;
-        float v = ha[o];
-        if (nh > 0) {
-          for (int q = 0; q < nh; ++q) {
-            const wf_source& S = P.src[L.h[q]];
-            if (src_hits(S, gi, gj)) v = fadd(v, src_value(S, gi, gj, n));
+    // (1) E-field soft injection on own cells, in collection order.
+    if (T.my_e) {
+      for (int s = 0; s < T.ne; ++s) {
+        const wf_source& Q = P.src[S.e[s]];
+        if (gj < Q.j0 || gj >= Q.j1) continue;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int gi = ri0 + r0 + q;
+          if (gi >= Q.i0 && gi < Q.i1) {
+            if (Q.comp == WF_EX) ex[q] = fadd(ex[q], src_value(Q, gi, gj, n));
+            else ey[q] = fadd(ey[q], src_value(Q, gi, gj, n));
           }
         }
-        if (gi < nx - 1 && gj < ny - 1 && r + 1 < RH && c + 1 < RW) {
-          const float t2 = fdiv(fsub(ex[o + 1], ex[o]), dy);
-          const float t4 = fdiv(fsub(ey[o + RW], ey[o]), dx);
-          v = fadd(v, fmul(dh, fsub(t2, t4)));
-        }
-        hb[o] = v;
       }
     }
+    // exchange for the Faraday update
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) S.xe[r0 + q][wx] = ex[q];
+    }
+    S.yr[wy][c] = ey[0];
     __syncthreads();
 
-    // (3) Mur edges.  X = value after the x-edge pass, F = after the y-edge
-    // pass.  X is only ever evaluated on columns that are not y-edges, so both
-    // read pre-step Hz (ha) and curl-updated Hz (hb) of NON-edge cells only:
-    // the edge writes below cannot race with these reads (needs Nx, Ny >= 3).
-    {
-      const bool top = (ri0 == 0), bot = (ri1 == nx), lef = (rj0 == 0), rig = (rj1 == ny);
-      auto X = [&](int r, int c) -> float {
+    // (2) Hz injection + Faraday curl.
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      float exr = __shfl_down_sync(0xffffffffu, ex[q], 1);
+      if (lane == 31) exr = (wx + 1 < WX) ? S.xe[r0 + q][wx + 1] : 0.f;
+      float eyb;
+      if (q + 1 < R) eyb = ey[q + 1];
+      else eyb = (wy + 1 < WY) ? S.yr[wy + 1][c] : 0.f;
+      const float t2 = divy(fsub(exr, ex[q]));
+      const float t4 = divx(fsub(eyb, ey[q]));
+      if (EDGE) S.sp[r0 + q][c] = hz[q];  // Mur snapshot (pre-injection)
+      float v = hz[q];
+      if (T.my_h) {
+        const int gi = ri0 + r0 + q;
+        for (int s = 0; s < T.nh; ++s) {
+          const wf_source& Q = P.src[S.h[s]];
+          if (gi >= Q.i0 && gi < Q.i1 && gj >= Q.j0 && gj < Q.j1) v = fadd(v, src_value(Q, gi, gj, n));
+        }
+      }
+      const float vc = fadd(v, fmul(dh, fsub(t2, t4)));
+      if (EDGE) {
+        const int gi = ri0 + r0 + q;
+        hz[q] = (curl_col && gi < nx - 1) ? vc : v;
+      } else {
+        hz[q] = vc;
+      }
+    }
+
+    // (3) Mur edges.
+    if (EDGE) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) S.sc[r0 + q][c] = hz[q];
+      __syncthreads();
+      // X: value after the x-edge pass, F: after the y-edge pass.  Only
+      // non-edge staged values are read, so the results can go straight back
+      // into registers (Nx, Ny >= 3).
+      const int RHa = T.RHa, RWa = T.RWa;
+      auto X = [&](int r, int cc) -> float {
         const int gi = ri0 + r;
-        if (gi == 0) return fadd(ha[RW + c], fmul(mx, fsub(hb[RW + c], ha[c])));
+        if (gi == 0) return fadd(S.sp[1][cc], fmul(mx, fsub(S.sc[1][cc], S.sp[0][cc])));
         if (gi == nx - 1)
-          return fadd(ha[(RH - 2) * RW + c],
-                      fmul(mx, fsub(hb[(RH - 2) * RW + c], ha[(RH - 1) * RW + c])));
-        return hb[r * RW + c];
+          return fadd(S.sp[RHa - 2][cc], fmul(mx, fsub(S.sc[RHa - 2][cc], S.sp[RHa - 1][cc])));
+        return S.sc[r][cc];
       };
-      auto F = [&](int r, int c) -> float {
-        const int gj = rj0 + c;
-        if (gj == 0) return fadd(ha[r * RW + 1], fmul(my, fsub(X(r, 1), ha[r * RW])));
-        if (gj == ny - 1)
-          return fadd(ha[r * RW + RW - 2], fmul(my, fsub(X(r, RW - 2), ha[r * RW + RW - 1])));
-        return X(r, c);
-      };
-      const int nrow = (top ? RW : 0) + (bot ? RW : 0);
-      const int cr0 = top ? 1 : 0, cr1 = bot ? RH - 1 : RH;
-      const int ncolr = cr1 - cr0;
-      const int ncol = (lef ? ncolr : 0) + (rig ? ncolr : 0);
-      for (int e = tid; e < nrow + ncol; e += blockDim.x) {
-        int r, c;
-        if (e < nrow) {
-          const bool first = top && e < RW;
-          r = first ? 0 : RH - 1;
-          c = first ? e : e - (top ? RW : 0);
-        } else {
-          const int e2 = e - nrow;
-          const bool first = lef && e2 < ncolr;
-          c = first ? 0 : RW - 1;
-          r = cr0 + (first ? e2 : e2 - (lef ? ncolr : 0));
-        }
-        hb[r * RW + c] = F(r, c);
-      }
-    }
-    __syncthreads();
-
-    // (4) Ampere updates (in place; each reads only its own Ex/Ey and hb).
-    for (int r = warp; r < RH; r += nw) {
-      const int gi = ri0 + r;
-      for (int c = lane; c < RW; c += 32) {
-        const int gj = rj0 + c;
-        const int o = r * RW + c;
-        if (gj >= 1 && c >= 1) {
-          const float d = fdiv(fsub(hb[o], hb[o - 1]), dy);
-          ex[o] = MAT ? fadd(fmul(ca[o], ex[o]), fmul(cb[o], d)) : fadd(ex[o], fmul(de, d));
-        }
-        if (gi >= 1 && r >= 1) {
-          const float d = fdiv(fsub(hb[o], hb[o - RW]), dx);
-          ey[o] = MAT ? fsub(fmul(ca[o], ey[o]), fmul(cb[o], d)) : fsub(ey[o], fmul(de, d));
+      if (colv) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int r = r0 + q, gi = ri0 + r;
+          if (r >= RHa) continue;
+          if (gj == 0) hz[q] = fadd(S.sp[r][1], fmul(my, fsub(X(r, 1), S.sp[r][0])));
+          else if (gj == ny - 1)
+            hz[q] = fadd(S.sp[r][RWa - 2], fmul(my, fsub(X(r, RWa - 2), S.sp[r][RWa - 1])));
+          else if (gi == 0 || gi == nx - 1) hz[q] = X(r, c);
         }
       }
     }
+
+    // exchange for the Ampere update
+    if (lane == 31) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) S.hx[r0 + q][wx] = hz[q];
+    }
+    S.hr[wy][c] = hz[R - 1];
     __syncthreads();
 
-    // (5) detectors (cells of the core) and stability maxima.
-    for (int q = tid; q < np; q += blockDim.x) {
-      const wf_probe& pr = P.prb[L.p[q]];
-      const int o = (pr.i - ri0) * RW + (pr.j - rj0);
-      const float v = pr.comp == WF_EX ? ex[o] : pr.comp == WF_EY ? ey[o] : hb[o];
-      P.traces[(long long)L.p[q] * P.trace_ld + (n - P.trace_step0)] = v;
+    // (4) Ampere updates.
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      float hl = __shfl_up_sync(0xffffffffu, hz[q], 1);
+      if (lane == 0) hl = (wx > 0) ? S.hx[r0 + q][wx - 1] : 0.f;
+      float ha;
+      if (q > 0) ha = hz[q - 1];
+      else ha = (wy > 0) ? S.hr[wy - 1][c] : 0.f;
+      const float d1 = divy(fsub(hz[q], hl));
+      const float d2 = divx(fsub(hz[q], ha));
+      const float nex = MAT ? fadd(fmul(ca[q], ex[q]), fmul(cb[q], d1)) : fadd(ex[q], fmul(de, d1));
+      const float ney = MAT ? fsub(fmul(ca[q], ey[q]), fmul(cb[q], d2)) : fsub(ey[q], fmul(de, d2));
+      if (EDGE) {
+        const int gi = ri0 + r0 + q;
+        ex[q] = ex_col ? nex : ex[q];
+        ey[q] = (gi >= 1) ? ney : ey[q];
+      } else {
+        ex[q] = nex;
+        ey[q] = ney;
+      }
+    }
+
+    // (5) detectors and stability maxima.
+    if (T.pown0 >= 0) {
+      auto sample = [&](int code) -> float {
+        const int rr = code / 3, cmp = code % 3;
+        float v = 0.f;
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+          if (q == rr) v = cmp == 0 ? ex[q] : (cmp == 1 ? ey[q] : hz[q]);
+        return v;
+      };
+      P.traces[(long long)T.pown0 * P.trace_ld + (n - P.trace_step0)] = sample(T.pq0);
+      if (T.pown1 >= 0)
+        P.traces[(long long)T.pown1 * P.trace_ld + (n - P.trace_step0)] = sample(T.pq1);
+      if (T.pslow) {
+        for (int s = 0; s < T.np; ++s) {
+          const int id = S.p[s];
+          if (id == T.pown0 || id == T.pown1) continue;
+          const wf_probe& pr = P.prb[id];
+          const int rr = pr.i - ri0 - r0;
+          if (pr.j == gj && rr >= 0 && rr < R)
+            P.traces[(long long)id * P.trace_ld + (n - P.trace_step0)] =
+                sample(rr * 3 + (pr.comp == WF_HZ ? 2 : pr.comp));
+        }
+      }
     }
     if (P.check_max != nullptr && P.n_check > 0 && (n + 1) % P.n_check == 0) {
       unsigned m0 = 0, m1 = 0, m2 = 0;
-      for (int i = ci0 + warp; i < ci1; i += nw)
-        for (int j = cj0 + lane; j < cj1; j += 32) {
-          const int o = (i - ri0) * RW + (j - rj0);
-          m0 = max(m0, abs_bits(ex[o]));
-          m1 = max(m1, abs_bits(ey[o]));
-          m2 = max(m2, abs_bits(hb[o]));
+      if (gj >= T.cj0 && gj < T.cj1) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int gi = ri0 + r0 + q;
+          if (gi >= T.ci0 && gi < T.ci1) {
+            m0 = max(m0, abs_bits(ex[q]));
+            m1 = max(m1, abs_bits(ey[q]));
+            m2 = max(m2, abs_bits(hz[q]));
+          }
         }
+      }
       for (int sh = 16; sh > 0; sh >>= 1) {
         m0 = max(m0, __shfl_xor_sync(0xffffffffu, m0, sh));
         m1 = max(m1, __shfl_xor_sync(0xffffffffu, m1, sh));
         m2 = max(m2, __shfl_xor_sync(0xffffffffu, m2, sh));
       }
       if (lane == 0) {
-        atomicMax(&L.bmax[0], m0);
-        atomicMax(&L.bmax[1], m1);
-        atomicMax(&L.bmax[2], m2);
+        atomicMax(&S.bmax[0], m0);
+        atomicMax(&S.bmax[1], m1);
+        atomicMax(&S.bmax[2], m2);
       }
       __syncthreads();
-      if (tid < 3) {
+      if (threadIdx.x < 3) {
         const int idx = (n + 1) / P.n_check - P.check_base - 1;
-        atomicMax(&P.check_max[idx * 3 + tid], L.bmax[tid]);
-        L.bmax[tid] = 0u;
+        atomicMax(&P.check_max[idx * 3 + threadIdx.x], S.bmax[threadIdx.x]);
+        S.bmax[threadIdx.x] = 0u;
       }
     }
-    float* tmp = ha;
-    ha = hb;
-    hb = tmp;
-    __syncthreads();
+  }
+}
+
+template <class C, bool MAT, bool FDIV>
+__device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int step0, int k,
+                       TileSmem<C>& S) {
+  constexpr int R = C::R, WX = C::WX;
+  const int nx = P.nx, ny = P.ny;
+  TileCtx T;
+  T.ci0 = ci0;
+  T.ci1 = ci1;
+  T.cj0 = cj0;
+  T.cj1 = cj1;
+  T.ri0 = max(ci0 - k, 0);
+  T.ri1 = min(ci1 + k, nx);
+  T.rj0 = max(cj0 - k, 0);
+  T.rj1 = min(cj1 + k, ny);
+  T.RHa = T.ri1 - T.ri0;
+  T.RWa = T.rj1 - T.rj0;
+  const int tid = threadIdx.x;
+  T.lane = tid & 31;
+  const int warp = tid >> 5;
+  T.wx = warp % WX;
+  T.wy = warp / WX;
+  T.c = T.wx * 32 + T.lane;
+  T.r0 = T.wy * R;
+  T.gj = T.rj0 + T.c;
+  const int ri0 = T.ri0, ri1 = T.ri1, rj0 = T.rj0, rj1 = T.rj1, r0 = T.r0, gj = T.gj;
+
+  // ---- local source / probe lists ------------------------------------------
+  if (tid == 0) {
+    int nh = 0, ne = 0;
+    for (int s = 0; s < P.nsrc; ++s) {
+      const wf_source& Q = P.src[s];
+      if (Q.i1 <= ri0 || Q.i0 >= ri1 || Q.j1 <= rj0 || Q.j0 >= rj1) continue;
+      if (Q.comp == WF_HZ) {
+        if (nh < kMaxLocalSrc) S.h[nh++] = (short)s;
+        else if (P.status) atomicExch(P.status, WF_E_LIMIT);
+      } else {
+        if (ne < kMaxLocalSrc) S.e[ne++] = (short)s;
+        else if (P.status) atomicExch(P.status, WF_E_LIMIT);
+      }
+    }
+    S.nh = nh;
+    S.ne = ne;
+    S.np = 0;
+    S.bmax[0] = S.bmax[1] = S.bmax[2] = 0u;
+  }
+  __syncthreads();
+  for (int q = tid; q < P.nprb; q += C::THREADS) {
+    const wf_probe& pr = P.prb[q];
+    if (pr.i >= ci0 && pr.i < ci1 && pr.j >= cj0 && pr.j < cj1) {
+      const int slot = atomicAdd(&S.np, 1);
+      if (slot < kMaxLocalProbe) S.p[slot] = (short)q;
+      else if (P.status) atomicExch(P.status, WF_E_LIMIT);
+    }
   }
 
-  // ---- store core ------------------------------------------------------
-  for (int i = ci0 + warp; i < ci1; i += nw) {
-    const long long g = (long long)i * ny;
-    for (int j = cj0 + lane; j < cj1; j += 32) {
-      const int o = (i - ri0) * RW + (j - rj0);
-      P.ex_out[g + j] = ex[o];
-      P.ey_out[g + j] = ey[o];
-      P.hz_out[g + j] = ha[o];
+  // ---- load own cells ----------------------------------------------------
+  float ex[R], ey[R], hz[R], ca[R], cb[R];
+  const bool colv = T.c < T.RWa;
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int r = r0 + q;
+    ex[q] = ey[q] = hz[q] = 0.f;
+    ca[q] = cb[q] = 0.f;
+    if (colv && r < T.RHa) {
+      const long long g = (long long)(ri0 + r) * ny + gj;
+      ex[q] = P.ex_in[g];
+      ey[q] = P.ey_in[g];
+      hz[q] = P.hz_in[g];
+      if (MAT) {
+        ca[q] = P.ca[g];
+        cb[q] = P.cb[g];
+      }
+    }
+  }
+  __syncthreads();
+  T.nh = S.nh;
+  T.ne = S.ne;
+  T.np = min(S.np, kMaxLocalProbe);
+  // Does any local source touch this thread's column segment?
+  T.my_h = false;
+  T.my_e = false;
+  for (int q = 0; q < T.nh; ++q) {
+    const wf_source& Q = P.src[S.h[q]];
+    T.my_h |= gj >= Q.j0 && gj < Q.j1 && ri0 + r0 < Q.i1 && ri0 + r0 + R > Q.i0;
+  }
+  for (int q = 0; q < T.ne; ++q) {
+    const wf_source& Q = P.src[S.e[q]];
+    T.my_e |= gj >= Q.j0 && gj < Q.j1 && ri0 + r0 < Q.i1 && ri0 + r0 + R > Q.i0;
+  }
+  // Probes owned by this thread (up to two in registers, else the slow path).
+  T.pown0 = T.pown1 = -1;
+  T.pq0 = T.pq1 = 0;
+  T.pslow = false;
+  for (int q = 0; q < T.np; ++q) {
+    const wf_probe& pr = P.prb[S.p[q]];
+    const int rr = pr.i - ri0 - r0;
+    if (pr.j == gj && rr >= 0 && rr < R) {
+      const int code = rr * 3 + (pr.comp == WF_HZ ? 2 : pr.comp);
+      if (T.pown0 < 0) {
+        T.pown0 = S.p[q];
+        T.pq0 = code;
+      } else if (T.pown1 < 0) {
+        T.pown1 = S.p[q];
+        T.pq1 = code;
+      } else {
+        T.pslow = true;
+      }
+    }
+  }
+  const bool edge_tile = (ri0 == 0) || (ri1 == nx) || (rj0 == 0) || (rj1 == ny);
+  if (edge_tile) tile2d_steps<C, MAT, FDIV, true>(P, T, S, ex, ey, hz, ca, cb, step0, k);
+  else tile2d_steps<C, MAT, FDIV, false>(P, T, S, ex, ey, hz, ca, cb, step0, k);
+
+  // ---- store core ----------------------------------------------------------
+  if (gj >= cj0 && gj < cj1) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int gi = ri0 + r0 + q;
+      if (gi >= ci0 && gi < ci1) {
+        const long long g = (long long)gi * ny + gj;
+        P.ex_out[g] = ex[q];
+        P.ey_out[g] = ey[q];
+        P.hz_out[g] = hz[q];
+      }
     }
   }
   __syncthreads();

@@ -20,6 +20,23 @@ __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 
+// Division of a float32 x by a float32 spacing d through float64:
+// q = RN32( RN64( (double)x * rd ) ) with rd = RN64(1/d).  The exact
+// quotient x/d of two 24-bit-significand numbers lies either exactly on, or
+// at least ~2^-48 (relative) away from, every float32 rounding midpoint (the
+// numerator of the difference is a non-zero integer multiple of the midpoint
+// spacing over d); for d not a power of two it is never exactly on one.  The
+// float64 product is within ~2^-52 of x/d, so its rounding to float32 equals
+// the correctly rounded IEEE quotient for every x, including subnormals,
+// zeros of either sign, infinities and NaN (the argument behind "innocuous"
+// double rounding, S. A. Figueroa 1995; J.-M. Muller et al., "Handbook of
+// Floating-Point Arithmetic", ch. on double rounding).  Because the engines'
+// bit-exactness rests on it, wf_check_fastdiv still compares it with
+// __fdiv_rn on all 2^32 inputs for each spacing before it is enabled.
+__device__ __forceinline__ float div_fast(float x, double rd) {
+  return __double2float_rn(__dmul_rn((double)x, rd));
+}
+
 // |x| as ordered bits: for non-negative floats the unsigned bit pattern is
 // monotone in the value, and NaN (0x7fc00000..) sorts above +inf, so a NaN
 // field shows up as "above any threshold" in the stability check.
