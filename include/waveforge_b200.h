@@ -141,6 +141,29 @@ int32_t wf_fdtd2d_run(const wf_grid2d* g,
                       int32_t n_check, uint32_t* check_max,
                       const wf_tune* tune, void* stream);
 
+/* Same as wf_fdtd2d_run, for callers that cannot allocate device memory
+ * (applications whose own pool allocator owns all GPU memory, or loops that
+ * must not call cudaMalloc/cudaFree because those can synchronise the
+ * device).  No counterpart in the reference: it only exists for such callers.
+ * The ping-pong scratch is a file-scope device array built into the library
+ * (3 x WF_NOALLOC_MAX_CELLS floats = 12 MiB, reserved on every GPU that loads
+ * the library until the process exits); grids above WF_NOALLOC_MAX_CELLS
+ * cells are rejected with WF_E_LIMIT.  Nothing is allocated.  The first call
+ * on each device looks the array's device address up once, so make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: calls that may overlap on the GPU race and must be serialised by
+ * the caller.  Nothing in the array needs to start at zero. */
+#define WF_NOALLOC_MAX_CELLS (1LL << 20)
+int32_t wf_fdtd2d_run_noalloc(const wf_grid2d* g,
+                              float* ex, float* ey, float* hz,
+                              const float* ca, const float* cb,
+                              const wf_source* src, int32_t nsrc,
+                              const wf_probe* probes, int32_t nprobe,
+                              float* traces, int64_t trace_ld, int32_t trace_step0,
+                              int32_t step0, int32_t nsteps,
+                              int32_t n_check, uint32_t* check_max,
+                              const wf_tune* tune, void* stream);
+
 /* Advance a 3D grid nsteps time steps.
  * Replaces FDTD3D.step/run (src/core/fdtd3d.py:261-516) with
  * MurABC3D.snapshot/apply (src/core/boundaries.py:488-583), source injection

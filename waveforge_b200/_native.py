@@ -22,7 +22,8 @@ WF_OK, WF_E_ARG, WF_E_CUDA, WF_E_LIMIT, WF_E_DIVERGED, WF_E_TIMEOUT = range(6)
 COMP_CODE = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
 
 EXPORTED = ("wf_abi_version", "wf_last_error", "wf_check_fastdiv", "wf_fdtd2d_run",
-            "wf_fdtd3d_run", "wf_batch2d_run", "wf_das2d")
+            "wf_fdtd2d_run_noalloc", "wf_fdtd3d_run", "wf_batch2d_run", "wf_das2d")
+NOALLOC_MAX_CELLS = 1 << 20   # WF_NOALLOC_MAX_CELLS of the header
 WF_FASTDIV_X, WF_FASTDIV_Y, WF_FASTDIV_Z = 1, 2, 4
 
 
@@ -95,6 +96,11 @@ def load() -> ctypes.CDLL:
         POINTER(WfGrid2D), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
         c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int32,
         c_int32, c_int32, c_int32, c_void_p, POINTER(WfTune), c_void_p]
+    lib.wf_fdtd2d_run_noalloc.restype = c_int32
+    lib.wf_fdtd2d_run_noalloc.argtypes = [
+        POINTER(WfGrid2D), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,
+        c_void_p, c_int32, c_void_p, c_int64, c_int32, c_int32, c_int32, c_int32, c_void_p,
+        POINTER(WfTune), c_void_p]
     lib.wf_fdtd3d_run.restype = c_int32
     lib.wf_fdtd3d_run.argtypes = [
         POINTER(WfGrid3D), POINTER(c_void_p), POINTER(c_void_p), c_void_p, c_void_p,
