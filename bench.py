@@ -272,15 +272,207 @@ def run_reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# single-solve workloads: plain 2D (4096^2 lossy ellipses) and 3D head (256^3)
+# ---------------------------------------------------------------------------
+
+def default_depth(workload, cells):
+    """Temporal block depth the library picks without a tune (fdtd2d.cu
+    default_tune2d; fdtd3d.cu uses single-step passes)."""
+    if workload == "head3d":
+        return 1
+    return 6 if cells >= 1024 * 1024 else 4
+
+
+def pass_launches(nsteps, k):
+    """Kernel launches of one run: the pass plan of wf_common.cuh PassPlan
+    (the first pass is split when the pass count is odd and it has >= 2
+    steps) plus a copy-back when the pass count stays odd."""
+    p0 = -(-nsteps // k)
+    split = 1 if (p0 % 2 == 1 and min(nsteps, k) >= 2) else 0
+    passes = p0 + split
+    return passes + (passes % 2)
+
+
+def build_single(args, dev):
+    """The solve of --workload plain2d / head3d: returns (sim, detectors,
+    host (ca, cb), device (ca, cb), wave, cells, bytes per cell-update, oracle factory)."""
+    import oracle
+    from waveforge_b200 import workloads as W
+    from waveforge_b200 import (FDTD2D, FDTD3D, Detectors, FieldSet, MurABC, MurABC3D,
+                                PointSource, SourceCollection, YeeGrid)
+    from waveforge_b200.core.materials import Material, MaterialMap, MaterialMap3D
+    from waveforge_b200.core.sources import GaussianDerivativePulse
+
+    if args.workload == "plain2d":
+        wl = W.LossyEllipses(n=args.side or 4096, steps=args.nsteps)
+        n = wl.n
+        gh = YeeGrid(n, n, wl.dx, wl.dx, courant=wl.courant, device="cpu")
+        mm = MaterialMap(gh, default=wl.background(Material))
+        wl.paint(mm, Material)
+        ca, cb = mm.build()
+        g = YeeGrid(n, n, wl.dx, wl.dx, courant=wl.courant, device=dev)
+        f = FieldSet(g)
+        wave = GaussianDerivativePulse(1e9).build(wl.steps, g.dt, dev)
+        i, j = wl.source
+        src = PointSource(_TableWave(wave), i, j, "Hz", grid=g, N_steps=wl.steps)
+        cad, cbd = ca.to(dev), cb.to(dev)
+        sim = FDTD2D(g, f, MurABC(g, f.Hz), SourceCollection([src]), Ca=cad, Cb=cbd)
+        det = Detectors(wl.receivers)
+
+        def make_oracle():
+            o = oracle.Oracle2D(n, n, wl.dx, wl.dx, gh.dt, ca[..., 0], cb[..., 0])
+            o.add_point_source("Hz", i, j, oracle.gauss_deriv_wave(wl.steps, gh.dt))
+            return o, [("Hz", a, b) for a, b in wl.receivers]
+
+        name = f"lossy_ellipses_{n}x{n}_{wl.steps}steps_16rx"
+        return sim, det, (ca, cb), (cad, cbd), wave, n * n, 32, make_oracle, name, "k2d_pass"
+
+    wl = W.Head3D(n=args.side or 256, steps=args.nsteps)
+    n = wl.n
+    gh = YeeGrid(n, n, wl.dx, wl.dx, Nz=n, dz=wl.dx, courant=wl.courant, device="cpu")
+    mm = MaterialMap3D(gh, default=wl.background(Material))
+    wl.paint(mm, Material)
+    ca, cb = mm.build3d()
+    g = YeeGrid(n, n, wl.dx, wl.dx, Nz=n, dz=wl.dx, courant=wl.courant, device=dev)
+    f = FieldSet(g)
+    wave = GaussianDerivativePulse(1e9).build(wl.steps, g.dt, dev)
+    i, j, k = wl.source
+    src = PointSource(_TableWave(wave), i, j, "Ez", k=k, grid=g, N_steps=wl.steps)
+    cad, cbd = ca.to(dev), cb.to(dev)
+    sim = FDTD3D(g, f, MurABC3D(g, f.Hx, f.Hy, f.Hz), SourceCollection([src]), Ca=cad, Cb=cbd)
+    det = Detectors([("Ez",) + tuple(r) for r in wl.receivers()])
+
+    def make_oracle():
+        o = oracle.Oracle3D(n, n, n, wl.dx, wl.dx, wl.dx, gh.dt, ca, cb)
+        o.add_point_source("Ez", i, j, oracle.gauss_deriv_wave(wl.steps, gh.dt), k=k)
+        return o, [("Ez",) + tuple(r) for r in wl.receivers()]
+
+    name = f"head3d_{n}^3_{wl.steps}steps_{wl.n_rx}rx"
+    return sim, det, (ca, cb), (cad, cbd), wave, n ** 3, 56, make_oracle, name, "k3d_pass"
+
+
+def cpu_single_sample(make_oracle, cells, max_steps, budget_s=12.0):
+    """Time the CPU port of the reference loop on the same solve until
+    ``budget_s`` of work (or the solve's last step); returns (Gcell-upd/s,
+    cores, sample text)."""
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    o, probes = make_oracle()
+    o.run(1, probes)   # warm-up
+    done, t = 0, 0.0
+    while t < budget_s and done + 6 <= max_steps:
+        t0 = time.perf_counter()
+        o.run(5, probes)
+        t += time.perf_counter() - t0
+        done += 5
+    return (cells * done / t / 1e9, threads,
+            f"the same solve, first {done + 1} steps with its receivers gathered per step "
+            f"({cells * done:.3e} cell-updates in {t:.1f} s)")
+
+
+def bench_single(args, ws, rank, local):
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sim, det, host_c, dev_c, wave, cells, bpc, make_oracle, name, kname = build_single(args, dev)
+    stream = torch.cuda.current_stream(dev)
+    nsteps = args.nsteps
+    upd = cells * nsteps
+
+    def one_step():
+        sim.reset()
+        return sim.run(nsteps, record=det)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clk = ClockSampler(local)
+    clk.start()
+    times = []
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        one_step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        times.append(a.elapsed_time(b))
+    barrier(ws)
+    clocks = clk.stop()
+    ms_step = reduce_max(sum(times) / len(times), ws, dev)
+    value = ws * upd / (ms_step * 1e-3) / 1e9
+
+    # e2e: coefficients and waveform from pinned host memory, traces back to the host
+    ca_h, cb_h = (c.pin_memory() for c in host_c)
+    wave_h = wave.cpu().pin_memory()
+    tr_h = torch.empty((len(det), nsteps), dtype=torch.float32, pin_memory=True)
+
+    def e2e_step():
+        dev_c[0].copy_(ca_h, non_blocking=True)
+        dev_c[1].copy_(cb_h, non_blocking=True)
+        wave.copy_(wave_h, non_blocking=True)
+        tr = one_step()
+        tr_h.copy_(tr, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    s2 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e2.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = reduce_max(s2.elapsed_time(e2), ws, dev) / args.steps
+    h2d = (ca_h.numel() + cb_h.numel() + wave_h.numel()) * 4
+    d2h = tr_h.numel() * 4
+
+    peak, peak_kind = measured_peaks()
+    achieved = bpc * upd / (ms_step * 1e-3) / 1e9
+    k = sim._tune.steps_per_pass if sim._tune is not None else None
+    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "bytes_per_cell_update": bpc,
+            "note": f"algorithmic bytes = {bpc} B x cell-updates / run time (all passes); "
+                    "temporal blocking re-uses tiles on chip, so frac may exceed 1"}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_single_sample(make_oracle, cells, nsteps, args.ref_budget)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        line = {
+            "metric": f"Gcell-upd/s ({args.workload}, fp32)", "value": value, "unit": UNIT,
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": name, "cell_updates_per_step": upd, "tune": k,
+                       "l2": "fields + coefficients > L2, no flush", "parallelism": f"replicas x{ws}"},
+            "e2e": {"value": ws * upd / (ms_e2e * 1e-3) / 1e9, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": args.steps * pass_launches(nsteps, k or default_depth(args.workload, cells)),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mimo", choices=["mimo", "plain2d", "head3d"],
+                    help="mimo: batched uneven breast MIMO (default, the headline metric); "
+                         "plain2d: one 4096^2 lossy 2D solve; head3d: one 256^3 head solve")
+    ap.add_argument("--side", type=int, default=None,
+                    help="grid side of plain2d (4096) / head3d (256)")
     ap.add_argument("--phantoms", type=int, default=64)
     ap.add_argument("--tx", type=int, default=16)
-    ap.add_argument("--nsteps", type=int, default=3000)
+    ap.add_argument("--nsteps", type=int, default=None,
+                    help="time steps per solve (mimo 3000, plain2d 2000, head3d 1500)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--ref-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -288,9 +480,15 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    if args.nsteps is None:
+        args.nsteps = {"mimo": 3000, "plain2d": 2000, "head3d": 1500}[args.workload]
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
+        barrier(ws)
+        return
+    if args.workload != "mimo":
+        bench_single(args, ws, rank, local)
         barrier(ws)
         return
 
