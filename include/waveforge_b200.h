@@ -216,6 +216,52 @@ int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve,
                        const wf_tune* tune, int32_t ctas_per_sm,
                        int32_t fastdiv, void* stream);
 
+/* Recompute and keep every state of nsteps forward steps: states holds
+ * nsteps+1 slots of three planes (Ex, Ey, Hz; 3*nx*ny floats per slot);
+ * slot 0 is the input, slot s+1 the state after step step0+s.  Same kernel
+ * and arithmetic as wf_fdtd2d_run, so each slot is bit-identical to the
+ * state wf_fdtd2d_run reaches.  No reference counterpart: the adjoint of
+ * the reverse pass needs E^n and H^{n+1} of every step of a checkpoint
+ * segment (the reference has no adjoint; its plan is
+ * docs/architecture/DIFFERENTIABLE_PHYSICS.md). */
+int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int32_t nsteps,
+                         const float* ca, const float* cb,
+                         const wf_source* src, int32_t nsrc, int32_t step0, void* stream);
+
+/* Reverse (adjoint) steps of the 2D TM update for
+ * L = 1/2 sum_{p,n} (trace_p[n] - target_p[n])^2, the traces being the
+ * detector samples of src/core/fdtd2d.py:187-266 recorded after each step.
+ * Runs steps n = step0+nsteps-1 down to step0:
+ *  states   nsteps+1 forward slots from wf_fdtd2d_states (slot s = state
+ *           before step step0+s)
+ *  lam      in: dL/d(state after step step0+nsteps) without the residual of
+ *           that step; out: dL/d(state before step0).  3 planes (aEx, aEy,
+ *           aHz).  lam_scratch: 3 planes of caller scratch.
+ *  resid    nprobe rows of resid_ld floats, trace - target; column
+ *           n - resid_step0 holds step n (added at the probe before step n
+ *           is reversed)
+ *  g_ca/g_cb  float64 accumulators of dL/dCa, dL/dCb (nx*ny each), required
+ *           with ca/cb.  No reference counterpart. */
+int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int32_t nsteps,
+                         const float* ca, const float* cb,
+                         const wf_probe* probes, int32_t nprobe,
+                         const float* resid, int64_t resid_ld, int32_t resid_step0,
+                         int32_t step0, float* lam, float* lam_scratch,
+                         double* g_ca, double* g_cb, void* stream);
+
+/* Per-cell lossy coefficients from float64 eps_r, sigma, evaluated as
+ * Material.ca / Material.cb (src/core/materials.py:61-82) in float64 and
+ * rounded to float32 as MaterialMap.build stores them (:200-252). */
+int32_t wf_material_coeffs(const double* eps_r, const double* sigma, int64_t n, double dt,
+                           float* ca, float* cb, void* stream);
+
+/* Chain rule of wf_material_coeffs: g_eps = scale * dL/deps_r and
+ * g_sigma = scale * dL/dsigma from the dL/dCa, dL/dCb accumulators
+ * (float64).  No reference counterpart. */
+int32_t wf_material_grad(const double* eps_r, const double* sigma, int64_t n, double dt,
+                         const double* g_ca, const double* g_cb, double scale,
+                         double* g_eps, double* g_sigma, void* stream);
+
 /* Delay-and-sum backprojection on the device, bit-identical to the reference
  * NumPy float64 path of examples/brain_mimo_imaging.py:211-266 (and its
  * variants through px/py, gate_start, skip_self).

@@ -19,3 +19,4 @@ from .fdtd_ref import (  # noqa: F401
     ricker_wave, Oracle2D, Oracle3D,
 )
 from .das_ref import das_backprojection_ref  # noqa: F401
+from . import adjoint_ref  # noqa: F401

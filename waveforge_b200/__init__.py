@@ -12,7 +12,8 @@ from .core import __all__ as _core_all
 from .detectors import Detectors
 from .imaging.das import das_backprojection, das_image_device
 from .batch import Batch2D, BatchSolve
+from .adjoint import FDTDMisfit, MisfitProblem2D, fdtd_misfit
 
 __all__ = list(_core_all) + ["Detectors", "das_backprojection", "das_image_device", "Batch2D",
-                             "BatchSolve"]
+                             "BatchSolve", "FDTDMisfit", "MisfitProblem2D", "fdtd_misfit"]
 __version__ = "0.1.0"

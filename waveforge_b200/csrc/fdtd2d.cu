@@ -162,3 +162,52 @@ extern "C" int32_t wf_fdtd2d_run(const wf_grid2d* g, float* ex, float* ey, float
   }
   return WF_OK;
 }
+
+extern "C" int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int32_t nsteps,
+                                    const float* ca, const float* cb, const wf_source* src,
+                                    int32_t nsrc, int32_t step0, void* stream) {
+  if (g == nullptr || states == nullptr)
+    return set_error(WF_E_ARG, "wf_fdtd2d_states: null grid/states pointer");
+  if (g->nx < 4 || g->ny < 4)
+    return set_error(WF_E_ARG, "wf_fdtd2d_states: grid %dx%d below the 4x4 stencil minimum",
+                     g->nx, g->ny);
+  if ((ca == nullptr) != (cb == nullptr))
+    return set_error(WF_E_ARG, "wf_fdtd2d_states: Ca and Cb must be given together");
+  if (nsteps < 0 || step0 < 0 || nsrc < 0 || (nsrc > 0 && src == nullptr))
+    return set_error(WF_E_ARG, "wf_fdtd2d_states: bad counts or null source array");
+  if (nsrc > 32767) return set_error(WF_E_LIMIT, "wf_fdtd2d_states: at most 32767 sources");
+  if (nsteps == 0) return WF_OK;
+  wf_tune t = default_tune2d(g->nx, g->ny);
+  t.steps_per_pass = 1;
+  if (int rc = check_tune2d(t)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  Tile2D P{};
+  P.nx = g->nx;
+  P.ny = g->ny;
+  P.dh = g->dh;
+  P.de = g->de;
+  P.dx = g->dx;
+  P.dy = g->dy;
+  P.mx = g->mur_x;
+  P.my = g->mur_y;
+  P.fastdiv = g->flags;
+  P.ca = ca;
+  P.cb = cb;
+  P.src = src;
+  P.nsrc = nsrc;
+  const bool fdiv = (g->flags & (WF_FASTDIV_X | WF_FASTDIV_Y)) == (WF_FASTDIV_X | WF_FASTDIV_Y);
+  const long long cells = (long long)g->nx * g->ny;
+  for (int s = 0; s < nsteps; ++s) {
+    float* in = states + (long long)s * 3 * cells;
+    float* out = in + 3 * cells;
+    P.ex_in = in;
+    P.ey_in = in + cells;
+    P.hz_in = in + 2 * cells;
+    P.ex_out = out;
+    P.ey_out = out + cells;
+    P.hz_out = out + 2 * cells;
+    const int rc = dispatch_cfg2d(t, LaunchPass{P, 1, step0 + s, st, ca != nullptr, fdiv});
+    if (rc) return rc;
+  }
+  return WF_OK;
+}
