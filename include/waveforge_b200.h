@@ -262,6 +262,37 @@ int32_t wf_material_grad(const double* eps_r, const double* sigma, int64_t n, do
                          const double* g_ca, const double* g_cb, double scale,
                          double* g_eps, double* g_sigma, void* stream);
 
+/* One region of a painted 2D material map (painter's order: later regions
+ * win).  Parameters are the float32-rounded Python floats of the host
+ * painter; `material` indexes the Ca/Cb table (0 = default material).
+ *  WF_REGION_CIRCLE   p = ci, cj, r*r         (MaterialMap.add_circle,
+ *                                              src/core/materials.py:143-163)
+ *  WF_REGION_RECT     p = i0, i1, j0, j1      (add_rectangle, :165-185)
+ *  WF_REGION_ELLIPSE  p = ci, cj, a, b        (axis-aligned ellipse)
+ *  WF_REGION_SHELL    p = outer ci,cj,a,b, inner ci,cj,a,b (outer & ~inner) */
+#define WF_REGION_CIRCLE  0
+#define WF_REGION_RECT    1
+#define WF_REGION_ELLIPSE 2
+#define WF_REGION_SHELL   3
+typedef struct wf_region2d {
+  int32_t kind;
+  int32_t material;
+  float p[8];
+} wf_region2d;
+
+/* Paint Ca/Cb (nx*ny float32 each) on the device, bit-identical to
+ * MaterialMap.build (src/core/materials.py:200-252) for the same regions.
+ * regions: device array; table_ca/cb: nmat float32 on the device.  Optional
+ * (both or neither): eps_r/sigma float64 planes painted from the float64
+ * tables table_eps/table_sigma (the adjoint's chain rule needs them).  A
+ * region whose material index is outside [0, nmat) paints the default and
+ * sets *status (device, nullable) to WF_E_ARG.  At most 1024 regions. */
+int32_t wf_paint2d(int32_t nx, int32_t ny, const wf_region2d* regions, int32_t nreg,
+                   const float* table_ca, const float* table_cb,
+                   const double* table_eps, const double* table_sigma, int32_t nmat,
+                   float* ca, float* cb, double* eps_r, double* sigma,
+                   int32_t* status, void* stream);
+
 /* Delay-and-sum backprojection on the device, bit-identical to the reference
  * NumPy float64 path of examples/brain_mimo_imaging.py:211-266 (and its
  * variants through px/py, gate_start, skip_self).

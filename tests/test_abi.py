@@ -49,6 +49,7 @@ STRUCTS = {
     "wf_tune": (nat.WfTune, ["steps_per_pass", "tile_k", "threads"]),
     "wf_solve2d": (nat.WfSolve2D, ["g", "ex", "sz", "cb", "traces", "trace_ld", "nsrc",
                                    "step0", "nsteps", "n_check", "status", "check_max"]),
+    "wf_region2d": (nat.WfRegion2D, ["kind", "material", "p"]),
 }
 
 
@@ -83,3 +84,19 @@ def test_argument_errors_need_no_gpu():
     assert b"4x4" in lib.wf_last_error()
     rc = lib.wf_das2d(None, None, 1, 1, None, None, None, 1, None, 1, 1.0, 1.0, 0, 0, None, None)
     assert rc == nat.WF_E_ARG
+
+
+def test_new_entry_points_validate_on_host():
+    lib = nat.load()
+    g = nat.WfGrid2D(3, 8, 1.0, 1.0, 1.0, 1.0, -0.5, -0.5, 0)
+    assert lib.wf_adjoint2d_run(ctypes.byref(g), 1, 1, None, None, None, 0, None, 0, 0, 0, 1, 1,
+                                None, None, None) == nat.WF_E_ARG
+    assert lib.wf_fdtd2d_states(ctypes.byref(g), 1, 1, None, None, None, 0, 0, None) == nat.WF_E_ARG
+    assert lib.wf_material_coeffs(None, None, 4, 1e-12, None, None, None) == nat.WF_E_ARG
+    assert lib.wf_material_grad(None, None, 4, 1e-12, None, None, 1.0, None, None, None) == nat.WF_E_ARG
+    assert lib.wf_paint2d(0, 4, None, 0, None, None, None, None, 1, None, None, None, None, None,
+                          None) == nat.WF_E_ARG
+    assert lib.wf_paint2d(4, 4, 1, 2000, 1, 1, None, None, 1, 1, 1, None, None, None,
+                          None) == nat.WF_E_LIMIT
+    assert lib.wf_paint2d(4, 4, 1, 2, 1, 1, None, None, 1, 1, 1, 1, None, None,
+                          None) == nat.WF_E_ARG

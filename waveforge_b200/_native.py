@@ -23,7 +23,8 @@ COMP_CODE = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
 
 EXPORTED = ("wf_abi_version", "wf_last_error", "wf_check_fastdiv", "wf_fdtd2d_run",
             "wf_fdtd2d_run_noalloc", "wf_fdtd3d_run", "wf_batch2d_run", "wf_fdtd2d_states",
-            "wf_adjoint2d_run", "wf_material_coeffs", "wf_material_grad", "wf_das2d")
+            "wf_adjoint2d_run", "wf_material_coeffs", "wf_material_grad", "wf_paint2d",
+            "wf_das2d")
 NOALLOC_MAX_CELLS = 1 << 20   # WF_NOALLOC_MAX_CELLS of the header
 WF_FASTDIV_X, WF_FASTDIV_Y, WF_FASTDIV_Z = 1, 2, 4
 
@@ -56,6 +57,10 @@ class WfSource(ctypes.Structure):
 
 class WfProbe(ctypes.Structure):
     _fields_ = [("comp", c_int32), ("i", c_int32), ("j", c_int32), ("k", c_int32)]
+
+
+class WfRegion2D(ctypes.Structure):
+    _fields_ = [("kind", c_int32), ("material", c_int32), ("p", c_float * 8)]
 
 
 class WfTune(ctypes.Structure):
@@ -123,6 +128,10 @@ def load() -> ctypes.CDLL:
     lib.wf_material_grad.restype = c_int32
     lib.wf_material_grad.argtypes = [c_void_p, c_void_p, c_int64, c_double, c_void_p, c_void_p,
                                      c_double, c_void_p, c_void_p, c_void_p]
+    lib.wf_paint2d.restype = c_int32
+    lib.wf_paint2d.argtypes = [c_int32, c_int32, c_void_p, c_int32, c_void_p, c_void_p, c_void_p,
+                               c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                               c_void_p]
     lib.wf_das2d.restype = c_int32
     lib.wf_das2d.argtypes = [c_void_p, c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_int32,
                              c_void_p, c_int32, c_double, c_double, c_int32, c_int32, c_void_p,

@@ -91,12 +91,45 @@ class MaterialMap:
         self._default = default or TISSUE_LIBRARY["free_space"]
         self._regions: list[Callable[[torch.Tensor, torch.Tensor], torch.Tensor]] = []
         self._materials: list[Material] = []
+        # typed description of each region for the device painter (None = custom mask)
+        self._prims: list = []
 
     def add_circle(self, center: tuple[float, float], radius: float, material: Material) -> "MaterialMap":
         ci, cj = float(center[0]), float(center[1])
         r2 = radius * radius
         self._regions.append(lambda I, J: ((I - ci) ** 2 + (J - cj) ** 2) <= r2)
         self._materials.append(material)
+        self._prims.append(("circle", (ci, cj, r2)))
+        return self
+
+    def add_ellipse(self, center: tuple[float, float], semi_axes: tuple[float, float],
+                    material: Material) -> "MaterialMap":
+        """Axis-aligned ellipse ((I-ci)/a)**2 + ((J-cj)/b)**2 <= 1 (the mask the
+        reference's phantom examples paint with add_custom)."""
+        ci, cj = float(center[0]), float(center[1])
+        a, b = float(semi_axes[0]), float(semi_axes[1])
+        self._regions.append(lambda I, J: ((I - ci) / a) ** 2 + ((J - cj) / b) ** 2 <= 1.0)
+        self._materials.append(material)
+        self._prims.append(("ellipse", (ci, cj, a, b)))
+        return self
+
+    def add_shell(self, center: tuple[float, float], outer: tuple[float, float],
+                  inner: tuple[float, float], material: Material,
+                  inner_center: tuple[float, float] | None = None) -> "MaterialMap":
+        """Cells inside the outer ellipse and outside the inner one (a skin or
+        skull layer)."""
+        ci, cj = float(center[0]), float(center[1])
+        ki, kj = (ci, cj) if inner_center is None else (float(inner_center[0]), float(inner_center[1]))
+        a, b = float(outer[0]), float(outer[1])
+        a2, b2 = float(inner[0]), float(inner[1])
+
+        def fn(I, J):
+            out = ((I - ci) / a) ** 2 + ((J - cj) / b) ** 2 <= 1.0
+            inn = ((I - ki) / a2) ** 2 + ((J - kj) / b2) ** 2 <= 1.0
+            return out & ~inn
+        self._regions.append(fn)
+        self._materials.append(material)
+        self._prims.append(("shell", (ci, cj, a, b, ki, kj, a2, b2)))
         return self
 
     def add_rectangle(self, i_range: tuple[int, int], j_range: tuple[int, int],
@@ -105,13 +138,76 @@ class MaterialMap:
         j0, j1 = j_range
         self._regions.append(lambda I, J: (I >= i0) & (I <= i1) & (J >= j0) & (J <= j1))
         self._materials.append(material)
+        self._prims.append(("rect", (float(i0), float(i1), float(j0), float(j1))))
         return self
 
     def add_custom(self, mask_fn: Callable[[torch.Tensor, torch.Tensor], torch.Tensor],
                    material: Material) -> "MaterialMap":
         self._regions.append(mask_fn)
         self._materials.append(material)
+        self._prims.append(None)
         return self
+
+    @property
+    def device_paintable(self) -> bool:
+        """True when every region is a circle, rectangle, ellipse or shell."""
+        return all(p is not None for p in self._prims)
+
+    def build_device(self, device=None, out: tuple | None = None,
+                     eps_sigma: tuple | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+        """``(Ca, Cb)`` painted by the CUDA painter (``wf_paint2d``), each
+        ``(Nx, Ny, 1)`` float32 on ``device`` (default ``grid.device``),
+        bit-identical to ``build()``.  Only the region list and the material
+        tables cross to the device.  ``out``: optional (Ca, Cb) tensors to
+        fill; ``eps_sigma``: optional float64 (eps_r, sigma) planes to fill
+        too.  The Ca <= 0 check runs on the material table (no device sync)."""
+        from .. import _native as nat
+        if not self.device_paintable:
+            raise ValueError("build_device needs circle/rectangle/ellipse/shell regions only "
+                             "(add_custom masks are host-only: use build())")
+        dev = torch.device(device if device is not None else self._grid.device)
+        if dev.type != "cuda":
+            raise RuntimeError("build_device paints on a CUDA device only (use build() on the host)")
+        nx, ny = self._grid.Nx, self._grid.Ny
+        dt = self._grid.dt
+        mats = [self._default, *self._materials]
+        tca = torch.tensor([m.ca(dt) for m in mats], dtype=torch.float32)
+        tcb = torch.tensor([m.cb(dt) for m in mats], dtype=torch.float32)
+        teps = torch.tensor([m.eps_r for m in mats], dtype=torch.float64)
+        tsig = torch.tensor([m.sigma for m in mats], dtype=torch.float64)
+        _check_ca(tca, three_d=False)
+        kinds = {"circle": 0, "rect": 1, "ellipse": 2, "shell": 3}
+        regs = (nat.WfRegion2D * max(1, len(self._prims)))()
+        for q, (kind, params) in enumerate(self._prims):
+            r = regs[q]
+            r.kind = kinds[kind]
+            r.material = q + 1
+            for t, v in enumerate(params):
+                r.p[t] = nat.f32(v)
+        rb = bytes(memoryview(regs).cast("B"))
+        nm = len(mats)
+        parts = [torch.frombuffer(bytearray(rb), dtype=torch.uint8), teps.view(torch.uint8),
+                 tsig.view(torch.uint8), tca.view(torch.uint8), tcb.view(torch.uint8)]
+        host = torch.cat(parts).pin_memory()
+        blob = host.to(dev, non_blocking=True)
+        base = blob.data_ptr()
+        o_eps = len(rb)                 # a multiple of 8 (40-byte regions)
+        o_sig = o_eps + 8 * nm
+        o_ca = o_sig + 8 * nm
+        o_cb = o_ca + 4 * nm
+        if out is None:
+            ca = torch.empty((nx, ny, 1), dtype=torch.float32, device=dev)
+            cb = torch.empty((nx, ny, 1), dtype=torch.float32, device=dev)
+        else:
+            ca, cb = out
+        e_ptr = s_ptr = None
+        if eps_sigma is not None:
+            e_ptr, s_ptr = eps_sigma[0].data_ptr(), eps_sigma[1].data_ptr()
+        lib = nat.load()
+        nat.check(lib.wf_paint2d(nx, ny, base, len(self._prims), base + o_ca, base + o_cb,
+                                 base + o_eps, base + o_sig, nm, ca.data_ptr(), cb.data_ptr(),
+                                 e_ptr, s_ptr, None, nat.stream_handle(dev)))
+        return ca, cb
 
     def _paint2d(self):
         nx, ny = self._grid.Nx, self._grid.Ny

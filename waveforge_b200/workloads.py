@@ -80,7 +80,7 @@ class LossyEllipses:
             a, b = (float(v) for v in rng.uniform(20 * s, 400 * s, 2))
             er = float(rng.uniform(1.0, 60.0))
             sg = float(rng.uniform(0.0, 1.5))
-            mm.add_custom(ellipse_mask(ci, cj, a, b), Material(f"ellipse{e}", er, sg))
+            mm.add_ellipse((ci, cj), (a, b), Material(f"ellipse{e}", er, sg))
 
     @staticmethod
     def background(Material):
@@ -121,11 +121,9 @@ class BreastPhantom:
     def paint(self, mm, Material, with_tumor: bool = True) -> None:
         c = self.side / 2.0
         A, B, sk = self.A, self.B, self.skin
-        outer = ellipse_mask(c, c, A, B)
-        inner = ellipse_mask(c, c, A - sk, B - sk)
-        mm.add_custom(lambda I, J: outer(I, J) & ~inner(I, J), Material("skin", 36.0, 0.8))
-        mm.add_custom(inner, Material("adipose", 5.0, 0.04))
-        mm.add_custom(ellipse_mask(c, c, A / 2.0, B / 2.0), Material("fibroglandular", 40.0, 0.8))
+        mm.add_shell((c, c), (A, B), (A - sk, B - sk), Material("skin", 36.0, 0.8))
+        mm.add_ellipse((c, c), (A - sk, B - sk), Material("adipose", 5.0, 0.04))
+        mm.add_ellipse((c, c), (A / 2.0, B / 2.0), Material("fibroglandular", 40.0, 0.8))
         if with_tumor:
             mm.add_circle(self.tumor_center, self.tumor_r, Material("tumor", 55.0, 1.0))
 
@@ -197,3 +195,78 @@ class Head3D:
     @staticmethod
     def background(Material):
         return Material("background", 10.0, 0.0)
+
+
+# ---------------------------------------------------------------------------
+# serving stream (Poisson requests of lossy phantoms, some with gradients)
+# ---------------------------------------------------------------------------
+
+_GD_PULSE = None
+
+
+def _pulse():
+    global _GD_PULSE
+    if _GD_PULSE is None:
+        from .core.sources import GaussianDerivativePulse
+        _GD_PULSE = GaussianDerivativePulse(1e9)
+    return _GD_PULSE
+
+
+def serving_request(side: int, steps: int, seed: int, *, n_ant: int = 16, gradient: bool = False,
+                    dx: float = 1e-3, courant: float = 0.5, n_ellipses: int = 64):
+    """One imaging request of the serving workload: a lossy-ellipse phantom
+    (the 4096^2 workload's generator scaled to ``side``) with a tumour disc,
+    ``n_ant`` antennas on a ring of radius 0.4*side (each one a transmitter
+    run, all of them receivers), a 1 GHz Gaussian-derivative Hz pulse.  With
+    ``gradient`` the request also carries the measured phantom: the same
+    with the tumour's eps_r + 15."""
+    from .core.grid import YeeGrid
+    from .core.materials import Material, MaterialMap
+    from .serving import ImagingRequest
+    grid = YeeGrid(side, side, dx, dx, courant=courant, device="cpu")
+    wl = LossyEllipses(n=side, steps=steps, seed=seed, n_ellipses=n_ellipses, dx=dx,
+                       courant=courant)
+    rng = np.random.default_rng(seed + 7919)
+    r = max(2.0, 0.03 * side)
+    c = side / 2.0
+    ti, tj = (float(v) for v in c + rng.uniform(-0.25, 0.25, 2) * side)
+
+    def phantom(tumor_eps: float):
+        mm = MaterialMap(grid, default=wl.background(Material))
+        wl.paint(mm, Material)
+        mm.add_circle((ti, tj), r, Material("tumor", tumor_eps, 1.0))
+        return mm
+
+    ant = ring_positions(n_ant, 0.4 * side, c, c, side, side)
+    return ImagingRequest(phantom(55.0), ant, ant, steps, _pulse(),
+                          target=phantom(70.0) if gradient else None, tag=(side, steps, seed))
+
+
+@dataclass
+class ServingStream:
+    """Poisson arrivals at ``rate``/s for ``duration`` s; side log-uniform in
+    [side_min, side_max], steps uniform in [steps_min, steps_max], ``n_ant``
+    transmitters each, a ``grad_fraction`` of them gradient requests."""
+    rate: float = 200.0
+    duration: float = 60.0
+    seed: int = 5
+    side_min: int = 128
+    side_max: int = 1024
+    steps_min: int = 1000
+    steps_max: int = 5000
+    n_ant: int = 16
+    grad_fraction: float = 0.1
+
+    def arrivals(self):
+        rng = np.random.default_rng(self.seed)
+        t, out, q = 0.0, [], 0
+        while True:
+            t += float(rng.exponential(1.0 / self.rate))
+            if t >= self.duration:
+                return out
+            side = int(round(math.exp(rng.uniform(math.log(self.side_min), math.log(self.side_max)))))
+            steps = int(rng.integers(self.steps_min, self.steps_max + 1))
+            grad = bool(rng.uniform() < self.grad_fraction)
+            out.append((t, serving_request(side, steps, self.seed * 100003 + q, n_ant=self.n_ant,
+                                           gradient=grad)))
+            q += 1
