@@ -458,15 +458,99 @@ def bench_single(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# serving: Poisson stream through the continuous-batching server
+# ---------------------------------------------------------------------------
+
+def _stream_stats(tickets, window_s):
+    from waveforge_b200.serving import request_work
+    done = [t for t in tickets if t.status == "done"]
+    lat = sorted(t.latency for t in done)
+
+    def pct(p):
+        return lat[min(len(lat) - 1, int(math.ceil(p * len(lat))) - 1)] if lat else None
+
+    upd = sum(request_work(t.request) for t in done)
+    solves = sum(len(t.request.transmitters) for t in done)
+    return {"served": len(done), "rejected": sum(t.status == "rejected" for t in tickets),
+            "gradient_served": sum(t.request.target is not None for t in done),
+            "p50_s": pct(0.50), "p99_s": pct(0.99),
+            "mean_s": statistics.mean(lat) if lat else None,
+            "solves_per_s": solves / window_s, "gcell_upd_per_s": upd / window_s / 1e9,
+            "window_s": window_s, "cell_updates": upd}
+
+
+def bench_serve(args, ws, rank, local):
+    from waveforge_b200 import workloads as W
+    from waveforge_b200.serving import Server, serve_one_at_a_time
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t_gen = time.perf_counter()
+    arrivals = W.ServingStream(rate=args.rate, duration=args.duration, seed=args.seed).arrivals()
+    log(f"[bench] {len(arrivals)} requests generated in {time.perf_counter() - t_gen:.1f}s")
+    warm = W.ServingStream(rate=20.0, duration=0.3, seed=args.seed + 1, side_max=256,
+                           steps_max=1200).arrivals()
+    for _ in range(args.warmup):
+        Server(dev, max_wait_s=args.max_wait).serve(warm)
+    serve_one_at_a_time(dev, warm[:2])
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clk = ClockSampler(local)
+    clk.start()
+    stats = srv = None
+    for _ in range(args.steps):
+        srv = Server(dev, chunk_steps=args.chunk, max_wait_s=args.max_wait,
+                     hbm_budget=args.hbm_budget * 1e9)
+        tickets = srv.serve(arrivals)
+        window = max(t.t_done for t in tickets if t.t_done is not None)
+        stats = _stream_stats(tickets, window)
+    clocks = clk.stop()
+    base = serve_one_at_a_time(dev, arrivals, max_wait_s=args.max_wait)
+    bwin = max(t.t_done for t in base if t.t_done is not None)
+    bstats = _stream_stats(base, bwin)
+    value = reduce_max(-stats["gcell_upd_per_s"], ws, dev) * -1.0   # slowest replica
+    if rank == 0:
+        line = {
+            "metric": "served Gcell-upd/s (continuous batching, Poisson stream, fp32)",
+            "value": value * ws, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": stats["window_s"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"serve_poisson{args.rate:g}_{args.duration:g}s_side128-1024_"
+                                   "steps1000-5000_16tx_grad10pct",
+                       "requests": len(arrivals), "hbm_budget_gb": args.hbm_budget,
+                       "chunk_steps": args.chunk, "max_wait_s": args.max_wait,
+                       "policy": "FIFO admission by HBM footprint and <= 3 solves/SM in flight; "
+                                 "reject at arrival when the estimated wait exceeds max_wait_s",
+                       "parallelism": f"replicas x{ws}"},
+            "latency_s": {"p50": stats["p50_s"], "p99": stats["p99_s"], "mean": stats["mean_s"]},
+            "serving": stats,
+            "one_at_a_time": bstats,
+            "served_over_one_at_a_time": stats["gcell_upd_per_s"] / bstats["gcell_upd_per_s"],
+            "e2e": {"value": value * ws, "unit": UNIT, "h2d_bytes_per_step": srv.h2d_bytes,
+                    "d2h_bytes_per_step": srv.d2h_bytes,
+                    "note": "requests enter as host objects (phantom region lists) and leave as "
+                            "pinned host traces/gradients: the served figure is end to end"},
+            "clocks": clocks, "gpu_launches": srv.launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mimo", choices=["mimo", "plain2d", "head3d"],
+    ap.add_argument("--workload", default="mimo", choices=["mimo", "plain2d", "head3d", "serve"],
                     help="mimo: batched uneven breast MIMO (default, the headline metric); "
-                         "plain2d: one 4096^2 lossy 2D solve; head3d: one 256^3 head solve")
+                         "plain2d: one 4096^2 lossy 2D solve; head3d: one 256^3 head solve; "
+                         "serve: Poisson request stream through the continuous-batching server")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
+    ap.add_argument("--max-wait", type=float, default=2.0, help="serve: wait bound (s)")
+    ap.add_argument("--chunk", type=int, default=64, help="serve: steps per launch")
+    ap.add_argument("--hbm-budget", type=float, default=60.0, help="serve: admission budget (GB)")
     ap.add_argument("--side", type=int, default=None,
                     help="grid side of plain2d (4096) / head3d (256)")
     ap.add_argument("--phantoms", type=int, default=64)
@@ -481,10 +565,16 @@ def main():
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     if args.nsteps is None:
-        args.nsteps = {"mimo": 3000, "plain2d": 2000, "head3d": 1500}[args.workload]
+        args.nsteps = {"mimo": 3000, "plain2d": 2000, "head3d": 1500, "serve": 0}[args.workload]
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
+        barrier(ws)
+        return
+    if args.workload == "serve":
+        if "--steps" not in sys.argv:
+            args.steps = 1   # one timed stream unless asked
+        bench_serve(args, ws, rank, local)
         barrier(ws)
         return
     if args.workload != "mimo":

@@ -153,6 +153,12 @@ class _Live:
         self.probes = ProbeTable([("Hz", int(i), int(j)) for i, j in req.receivers], dev,
                                  _ALLOWED, (g.Nx, g.Ny, 1))
         self.g = grid_struct(g, dev)
+        # host->device bytes of admission: region lists + material tables per
+        # painted map, the source and probe descriptors
+        maps = [req.material] + ([req.target] if self.grad else [])
+        self.h2d = sum(len(m._prims) * ctypes.sizeof(nat.WfRegion2D) + 24 * (len(m._prims) + 1)
+                       for m in maps)
+        self.h2d += self.ntx * ctypes.sizeof(nat.WfSource) + self.nrx * ctypes.sizeof(nat.WfProbe)
         both = nat.WF_FASTDIV_X | nat.WF_FASTDIV_Y
         self.fast = (self.g.flags & both) == both
         self.desc = []
@@ -182,7 +188,8 @@ class Server:
     """Continuous-batching server on one device (see the module docstring)."""
 
     def __init__(self, device, *, hbm_budget: float = 60e9, chunk_steps: int = 64,
-                 max_wait_s: Optional[float] = None, tune=None, ctas_per_sm: int = 0) -> None:
+                 max_wait_s: Optional[float] = None, max_active_solves: Optional[int] = None,
+                 tune=None, ctas_per_sm: int = 0) -> None:
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("Server runs on a CUDA device only (no CPU fallback)")
@@ -190,6 +197,10 @@ class Server:
         if chunk_steps < 1:
             raise ValueError("chunk_steps must be >= 1")
         self.budget = int(hbm_budget)
+        # the persistent kernel runs one CTA per solve: a few solves per SM
+        # fill the GPU; admitting more only stretches every request's latency
+        nsm = torch.cuda.get_device_properties(self.device).multi_processor_count
+        self.max_active = int(max_active_solves) if max_active_solves else 3 * nsm
         self.chunk = int(chunk_steps)
         self.max_wait_s = max_wait_s
         self.tune = None if tune is None else nat.WfTune(*tune)
@@ -210,6 +221,8 @@ class Server:
         self.rate = 5e10            # cell-updates/s estimate for the wait bound (updated live)
         self.launches = 0
         self.cell_updates = 0
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
         self._chunk_events: list = []
         torch.cuda.synchronize(self.device)
         self.t0 = time.perf_counter()
@@ -261,14 +274,20 @@ class Server:
 
     # ------------------------------------------------------------------
     def _admit(self) -> None:
+        active = sum(L.nsol for L in self.live)
         while self.queue:
             tk = self.queue[0]
             fp = request_footprint(tk.request, self.chunk)
+            nsol = len(tk.request.transmitters) * (2 if tk.request.target is not None else 1)
             if self.used + fp > self.budget:
                 break   # arrival order: the head waits for memory
+            if self.live and active + nsol > self.max_active:
+                break   # the GPU is full: the head waits for a slot
+            active += nsol
             self.queue.pop(0)
             L = _Live(self, tk)
             self.used += L.bytes
+            self.h2d_bytes += L.h2d
             tk.status, tk.t_admit = "running", self.now()
             self.live.append(L)
 
@@ -294,6 +313,7 @@ class Server:
         order = sorted(range(n), key=lambda q: -sizes[q])
         host = torch.cat([raw, torch.tensor(order, dtype=torch.int32).view(torch.uint8)]).pin_memory()
         dev = host.to(self.device, non_blocking=True)
+        self.h2d_bytes += host.numel()
         self._keep = dev
         self._queue_ctr.zero_()
         fast = all(L.fast for L in self.live)
@@ -315,6 +335,7 @@ class Server:
         if not L.grad:
             L.host_traces = torch.empty((L.ntx, L.nrx, L.N), dtype=torch.float32, pin_memory=True)
             L.host_traces.copy_(L.traces, non_blocking=True)
+            self.d2h_bytes += L.host_traces.numel() * 4
             L.event = torch.cuda.Event(enable_timing=True)
             L.event.record(self.stream)
             self.retiring.append(L)
@@ -368,6 +389,7 @@ class Server:
         L.host_grad[0].copy_(geps, non_blocking=True)
         L.host_grad[1].copy_(gsig, non_blocking=True)
         L.host_grad[2, :1].copy_(loss.reshape(1), non_blocking=True)
+        self.d2h_bytes += L.host_traces.numel() * 4 + (2 * cells + 1) * 8
         L.adj_keep = (resid, gca, gcb, states, lam, lam_s, geps, gsig)
         L.event = torch.cuda.Event(enable_timing=True)
         L.event.record(self.side)
