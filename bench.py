@@ -62,7 +62,7 @@ def measured_peaks():
 # workload
 # ---------------------------------------------------------------------------
 
-def build_workload(dev, n_phantoms, n_tx, steps, seed):
+def build_workload(dev, n_phantoms, n_tx, steps, seed, mode="persistent", tune=None):
     from waveforge_b200 import (Batch2D, BatchSolve, Detectors, PointSource, SourceCollection,
                                 YeeGrid)
     from waveforge_b200.core.materials import Material, MaterialMap
@@ -93,7 +93,7 @@ def build_workload(dev, n_phantoms, n_tx, steps, seed):
                 src = PointSource(_TableWave(waves[ph.side]), i, j, "Hz", grid=g, N_steps=steps)
                 solves[tumor].append(BatchSolve(g, SourceCollection([src]), Detectors(ant), cad, cbd,
                                                 tag=(p, tx)))
-    batches = {t: Batch2D(solves[t], steps) for t in (True, False)}
+    batches = {t: Batch2D(solves[t], steps, mode=mode, tune=tune) for t in (True, False)}
     return wl, phantoms, batches, host_coeffs, dev_coeffs, waves
 
 
@@ -486,7 +486,8 @@ def bench_serve(args, ws, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     t_gen = time.perf_counter()
-    arrivals = W.ServingStream(rate=args.rate, duration=args.duration, seed=args.seed).arrivals()
+    arrivals = W.ServingStream(rate=args.rate, duration=args.duration, seed=args.seed,
+                               grad_fraction=args.grad_fraction).arrivals()
     log(f"[bench] {len(arrivals)} requests generated in {time.perf_counter() - t_gen:.1f}s")
     warm = W.ServingStream(rate=20.0, duration=0.3, seed=args.seed + 1, side_max=256,
                            steps_max=1200).arrivals()
@@ -500,7 +501,7 @@ def bench_serve(args, ws, rank, local):
     stats = srv = None
     for _ in range(args.steps):
         srv = Server(dev, chunk_steps=args.chunk, max_wait_s=args.max_wait,
-                     hbm_budget=args.hbm_budget * 1e9)
+                     hbm_budget=args.hbm_budget * 1e9, max_active_cells=args.max_cells)
         tickets = srv.serve(arrivals)
         window = max(t.t_done for t in tickets if t.t_done is not None)
         stats = _stream_stats(tickets, window)
@@ -546,11 +547,16 @@ def main():
                     help="mimo: batched uneven breast MIMO (default, the headline metric); "
                          "plain2d: one 4096^2 lossy 2D solve; head3d: one 256^3 head solve; "
                          "serve: Poisson request stream through the continuous-batching server")
+    ap.add_argument("--batch-mode", default="persistent", choices=["persistent", "tiled"],
+                    help="mimo: one persistent launch per batch, or one tile-queue launch per pass")
+    ap.add_argument("--tune", default=None, help="mimo: K,tile_i,tile_j,1,0 of the batched kernel")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
     ap.add_argument("--max-wait", type=float, default=2.0, help="serve: wait bound (s)")
-    ap.add_argument("--chunk", type=int, default=64, help="serve: steps per launch")
+    ap.add_argument("--chunk", type=int, default=128, help="serve: steps per chunk")
     ap.add_argument("--hbm-budget", type=float, default=60.0, help="serve: admission budget (GB)")
+    ap.add_argument("--grad-fraction", type=float, default=0.1, help="serve: gradient requests")
+    ap.add_argument("--max-cells", type=float, default=3.2e7, help="serve: in-flight cell cap")
     ap.add_argument("--side", type=int, default=None,
                     help="grid side of plain2d (4096) / head3d (256)")
     ap.add_argument("--phantoms", type=int, default=64)
@@ -585,8 +591,9 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     t_setup = time.perf_counter()
+    tune = None if args.tune is None else tuple(int(v) for v in args.tune.split(","))
     wl, phantoms, batches, host_coeffs, dev_coeffs, waves = build_workload(
-        dev, args.phantoms, args.tx, args.nsteps, args.seed)
+        dev, args.phantoms, args.tx, args.nsteps, args.seed, args.batch_mode, tune)
     images = torch.zeros((len(phantoms), DAS_SIZE, DAS_SIZE), dtype=torch.float64, device=dev)
     cells_per_step = 2 * batches[True].cells * args.nsteps   # both twins
     log(f"[bench] setup {time.perf_counter() - t_setup:.1f}s, {2 * len(batches[True].solves)} solves, "
@@ -719,15 +726,18 @@ def main():
     k_ms = statistics.mean(kern_ms)
     achieved = BYTES_PER_CELL_UPDATE * (cells_per_step / 2) / (k_ms * 1e-3) / 1e9
     traffic = None
-    tfile = ROOT / "profiles" / "k_batch2d_traffic.txt"
+    tfile = ROOT / "profiles" / ("k_batch2d_traffic.txt" if args.batch_mode == "persistent"
+                                 else "k_batch_pass_traffic.txt")
     if tfile.exists():
         for line in tfile.read_text().splitlines():
             if line.startswith("dram_bytes_per_cell_update="):
                 traffic = float(line.split("=")[1]) * cells_per_step / 2
-    roof = {"bound": "hbm", "kernel": "k_batch2d", "achieved": achieved, "peak": peak,
+    kname = "k_batch2d" if args.batch_mode == "persistent" else "k_batch_pass"
+    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
             "bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
-            "launch_ms": k_ms, "note": "algorithmic bytes = 32 B x cell-updates of one launch; "
+            "launch_ms": k_ms, "note": "algorithmic bytes = 32 B x cell-updates of one batch run "
+                                       "(persistent: one launch; tiled: all its pass launches); "
                                        "temporal blocking re-uses tiles on chip, so frac may exceed 1"}
 
     cpu = None
@@ -745,11 +755,12 @@ def main():
                        "twins": "tumour + healthy", "das": f"{len(phantoms)} x {DAS_SIZE}x{DAS_SIZE}",
                        "cell_updates_per_step": cells_per_step, "grid_sides": "150-512",
                        "dx_mm": 0.5, "courant": 0.5, "l2": "inputs > L2 (2.6 GB fields), no flush",
+                       "batch_mode": args.batch_mode, "tune": args.tune,
                        "parallelism": f"replicas x{ws}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
             "plain_per_solve": plain, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": args.steps * (2 + len(phantoms)),
+            "gpu_launches": args.steps * (2 * batches[True].launches_per_run() + len(phantoms)),
         }
         print(json.dumps(line), flush=True)
     barrier(ws)

@@ -216,37 +216,54 @@ int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve,
                        const wf_tune* tune, int32_t ctas_per_sm,
                        int32_t fastdiv, void* stream);
 
-/* Recompute and keep every state of nsteps forward steps: states holds
- * nsteps+1 slots of three planes (Ex, Ey, Hz; 3*nx*ny floats per slot);
- * slot 0 is the input, slot s+1 the state after step step0+s.  Same kernel
- * and arithmetic as wf_fdtd2d_run, so each slot is bit-identical to the
- * state wf_fdtd2d_run reaches.  No reference counterpart: the adjoint of
- * the reverse pass needs E^n and H^{n+1} of every step of a checkpoint
- * segment (the reference has no adjoint; its plan is
- * docs/architecture/DIFFERENTIABLE_PHYSICS.md). */
-int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int32_t nsteps,
-                         const float* ca, const float* cb,
-                         const wf_source* src, int32_t nsrc, int32_t step0, void* stream);
+/* One temporal pass of many solves, spread over the GPU by tiles.
+ * items: nitems (solve index, ci0, cj0) int32 triplets on the device, one
+ * CTA each: the core tile [ci0, ci0+tile_i-2k) x [cj0, cj0+tile_j-2k) of
+ * solve `solves[index]` advances k steps from step solves[index].step0 +
+ * step_offset, reading its state buffers (parity 0) or its scratch buffers
+ * (parity 1) and writing the other set.  Same tile routine as wf_fdtd2d_run,
+ * so a solve advanced by a sequence of these passes is bit-identical to its
+ * plain run with the same pass plan.  tune: region shape only (tile_i,
+ * tile_j; NULL = 48x128); fastdiv as in wf_batch2d_run.  Batching many
+ * solves is new; the reference runs them one FDTD2D at a time
+ * (examples/brain_mimo_imaging.py:176-204). */
+int32_t wf_batch2d_pass(const wf_solve2d* solves, const int32_t* items, int32_t nitems,
+                        int32_t parity, int32_t step_offset, int32_t k,
+                        const wf_tune* tune, int32_t fastdiv, void* stream);
+
+/* Recompute and keep every state of nsteps forward steps, for ntx runs that
+ * share the grid and the coefficients (e.g. the transmitters of one
+ * phantom).  Run t owns states + t*tx_stride: nsteps+1 slots of three planes
+ * (Ex, Ey, Hz; 3*nx*ny floats per slot); slot 0 is its input, slot s+1 the
+ * state after step step0+s; it uses sources [t*src_per_tx, (t+1)*src_per_tx).
+ * One launch per step covers every run.  Same tile routine and arithmetic
+ * as wf_fdtd2d_run, so each slot is bit-identical to the state
+ * wf_fdtd2d_run reaches.  No reference counterpart: the adjoint needs E^n
+ * and H^{n+1} of every step of a checkpoint segment (the reference has no
+ * adjoint; its plan is docs/architecture/DIFFERENTIABLE_PHYSICS.md). */
+int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int64_t tx_stride, int32_t ntx,
+                         int32_t nsteps, const float* ca, const float* cb,
+                         const wf_source* src, int32_t src_per_tx, int32_t step0, void* stream);
 
 /* Reverse (adjoint) steps of the 2D TM update for
  * L = 1/2 sum_{p,n} (trace_p[n] - target_p[n])^2, the traces being the
- * detector samples of src/core/fdtd2d.py:187-266 recorded after each step.
- * Runs steps n = step0+nsteps-1 down to step0:
- *  states   nsteps+1 forward slots from wf_fdtd2d_states (slot s = state
- *           before step step0+s)
- *  lam      in: dL/d(state after step step0+nsteps) without the residual of
- *           that step; out: dL/d(state before step0).  3 planes (aEx, aEy,
- *           aHz).  lam_scratch: 3 planes of caller scratch.
- *  resid    nprobe rows of resid_ld floats, trace - target; column
- *           n - resid_step0 holds step n (added at the probe before step n
- *           is reversed)
- *  g_ca/g_cb  float64 accumulators of dL/dCa, dL/dCb (nx*ny each), required
- *           with ca/cb.  No reference counterpart. */
-int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int32_t nsteps,
-                         const float* ca, const float* cb,
+ * detector samples of src/core/fdtd2d.py:187-266 recorded after each step,
+ * for ntx runs at once.  Runs steps n = step0+nsteps-1 down to step0:
+ *  states   run t: states + t*states_stride, the nsteps+1 slots of
+ *           wf_fdtd2d_states (slot s = state before step step0+s)
+ *  lam      ntx x 3 planes (aEx, aEy, aHz per run).  In: dL/d(state after
+ *           step step0+nsteps) without that step's residual; out: dL/d(state
+ *           before step0).  lam_scratch: the same size, caller scratch.
+ *  resid    run t: resid + t*resid_stride, nprobe rows of resid_ld floats
+ *           (trace - target); column n - resid_step0 holds step n
+ *  g_ca/g_cb  float64 accumulators of dL/dCa, dL/dCb, one nx*ny plane per run
+ *           (ntx planes each), required with ca/cb.  No reference
+ *           counterpart. */
+int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int64_t states_stride,
+                         int32_t ntx, int32_t nsteps, const float* ca, const float* cb,
                          const wf_probe* probes, int32_t nprobe,
-                         const float* resid, int64_t resid_ld, int32_t resid_step0,
-                         int32_t step0, float* lam, float* lam_scratch,
+                         const float* resid, int64_t resid_ld, int64_t resid_stride,
+                         int32_t resid_step0, int32_t step0, float* lam, float* lam_scratch,
                          double* g_ca, double* g_cb, void* stream);
 
 /* Per-cell lossy coefficients from float64 eps_r, sigma, evaluated as
@@ -256,10 +273,11 @@ int32_t wf_material_coeffs(const double* eps_r, const double* sigma, int64_t n, 
                            float* ca, float* cb, void* stream);
 
 /* Chain rule of wf_material_coeffs: g_eps = scale * dL/deps_r and
- * g_sigma = scale * dL/dsigma from the dL/dCa, dL/dCb accumulators
- * (float64).  No reference counterpart. */
+ * g_sigma = scale * dL/dsigma from `count` consecutive planes of dL/dCa,
+ * dL/dCb accumulators (float64, summed in plane order).  No reference
+ * counterpart. */
 int32_t wf_material_grad(const double* eps_r, const double* sigma, int64_t n, double dt,
-                         const double* g_ca, const double* g_cb, double scale,
+                         const double* g_ca, const double* g_cb, int32_t count, double scale,
                          double* g_eps, double* g_sigma, void* stream);
 
 /* One region of a painted 2D material map (painter's order: later regions

@@ -89,11 +89,20 @@ def test_argument_errors_need_no_gpu():
 def test_new_entry_points_validate_on_host():
     lib = nat.load()
     g = nat.WfGrid2D(3, 8, 1.0, 1.0, 1.0, 1.0, -0.5, -0.5, 0)
-    assert lib.wf_adjoint2d_run(ctypes.byref(g), 1, 1, None, None, None, 0, None, 0, 0, 0, 1, 1,
-                                None, None, None) == nat.WF_E_ARG
-    assert lib.wf_fdtd2d_states(ctypes.byref(g), 1, 1, None, None, None, 0, 0, None) == nat.WF_E_ARG
+    assert lib.wf_adjoint2d_run(ctypes.byref(g), 1, 0, 1, 1, None, None, None, 0, None, 0, 0, 0,
+                                0, 1, 1, None, None, None) == nat.WF_E_ARG
+    g8 = nat.WfGrid2D(8, 8, 1.0, 1.0, 1.0, 1.0, -0.5, -0.5, 0)
+    # several runs need a stride that holds a whole run's slots
+    assert lib.wf_adjoint2d_run(ctypes.byref(g8), 1, 10, 2, 1, None, None, None, 0, None, 0, 0, 0,
+                                0, 1, 1, None, None, None) == nat.WF_E_ARG
+    assert lib.wf_fdtd2d_states(ctypes.byref(g), 1, 0, 1, 1, None, None, None, 0, 0,
+                                None) == nat.WF_E_ARG
+    assert lib.wf_fdtd2d_states(ctypes.byref(g8), 1, 10, 2, 1, None, None, None, 0, 0,
+                                None) == nat.WF_E_ARG
     assert lib.wf_material_coeffs(None, None, 4, 1e-12, None, None, None) == nat.WF_E_ARG
-    assert lib.wf_material_grad(None, None, 4, 1e-12, None, None, 1.0, None, None, None) == nat.WF_E_ARG
+    assert lib.wf_material_grad(None, None, 4, 1e-12, None, None, 1, 1.0, None, None,
+                                None) == nat.WF_E_ARG
+    assert lib.wf_material_grad(1, 1, 4, 1e-12, 1, 1, 0, 1.0, 1, 1, None) == nat.WF_E_ARG
     assert lib.wf_paint2d(0, 4, None, 0, None, None, None, None, 1, None, None, None, None, None,
                           None) == nat.WF_E_ARG
     assert lib.wf_paint2d(4, 4, 1, 2000, 1, 1, None, None, 1, 1, 1, None, None, None,

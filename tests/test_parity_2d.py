@@ -143,14 +143,19 @@ def test_breast_mimo_alone_and_batched_bit_exact(cuda):
                                      ca.reshape(ph.side, ph.side, 1).to(cuda),
                                      cb.reshape(ph.side, ph.side, 1).to(cuda)))
             keys.append(f"p{p}_tx{tx}")
-    for tune in (None, (3, 32, 64, 1, 0), (6, 48, 128, 1, 0), (2, 8, 32, 1, 0)):
-        batch = Batch2D(solves, steps, tune=tune)
-        batch.run()
-        torch.cuda.synchronize()
-        assert all(s == 0 for s in batch.statuses())
-        for q, key in enumerate(keys):
-            assert sha(batch.traces(q)) == str(g[key + "_sha_traces"]), (tune, key)
-            assert sha(batch.fields(q)[2]) == str(g[key + "_sha_hz"]), (tune, key)
+    for mode in ("persistent", "tiled"):
+        for tune in (None, (3, 32, 64, 1, 0), (6, 48, 128, 1, 0), (2, 8, 32, 1, 0)):
+            batch = Batch2D(solves, steps, tune=tune, mode=mode)
+            if mode == "tiled":
+                for chunk in (7, 100, 1, steps - 108):   # uneven chunks, a single-step pass
+                    batch.run(chunk)
+            else:
+                batch.run()
+            torch.cuda.synchronize()
+            assert all(s == 0 for s in batch.statuses())
+            for q, key in enumerate(keys):
+                assert sha(batch.traces(q)) == str(g[key + "_sha_traces"]), (mode, tune, key)
+                assert sha(batch.fields(q)[2]) == str(g[key + "_sha_hz"]), (mode, tune, key)
 
 
 def _random_case(rng, nx, ny, steps, material, n_src):

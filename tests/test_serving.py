@@ -33,16 +33,17 @@ def test_footprint_and_work_accounting():
 
 
 @pytest.mark.gpu
-def test_forward_request_same_alone_in_mix_and_one_at_a_time(cuda):
+@pytest.mark.parametrize("mode", ["tiled", "persistent"])
+def test_forward_request_same_alone_in_mix_and_one_at_a_time(cuda, mode):
     probe = _req(72, 150, 7)
-    alone = Server(cuda, chunk_steps=32)
+    alone = Server(cuda, chunk_steps=32, mode=mode)
     tk = alone.submit(probe)
     alone.drain()
     assert tk.status == "done"
     ref = tk.traces.clone()
     assert float(ref.abs().max()) > 0
 
-    mix = Server(cuda, chunk_steps=32)
+    mix = Server(cuda, chunk_steps=32, mode=mode, max_active_cells=2e5)
     others = [_req(s, n, 100 + s) for s, n in ((96, 200), (48, 90), (130, 260), (64, 40))]
     tks = [mix.submit(r) for r in others[:2]]
     mix.step()
@@ -59,15 +60,16 @@ def test_forward_request_same_alone_in_mix_and_one_at_a_time(cuda):
 
 
 @pytest.mark.gpu
-def test_gradient_request_same_alone_in_mix_and_one_at_a_time(cuda):
+@pytest.mark.parametrize("mode", ["tiled", "persistent"])
+def test_gradient_request_same_alone_in_mix_and_one_at_a_time(cuda, mode):
     g = _req(64, 120, 3, grad=True, n_ant=4)
-    alone = Server(cuda, chunk_steps=16)
+    alone = Server(cuda, chunk_steps=16, mode=mode)
     tk = alone.submit(g)
     alone.drain()
     assert tk.status == "done" and tk.grad_eps is not None
     assert float(tk.grad_eps.abs().max()) > 0 and tk.loss > 0
 
-    mix = Server(cuda, chunk_steps=16)
+    mix = Server(cuda, chunk_steps=16, mode=mode)
     first = [mix.submit(_req(80, 150, 21)), mix.submit(_req(50, 60, 22, grad=True, n_ant=4))]
     mix.step()
     tk2 = mix.submit(g)

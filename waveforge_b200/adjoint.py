@@ -17,8 +17,9 @@ forward, same kernel), ``wf_adjoint2d_run`` runs the time-reversed Yee steps
 that carry dL/dstate backwards and accumulate dL/dCa, dL/dCb in float64, and
 ``wf_material_grad`` applies the chain rule to dL/deps_r, dL/dsigma.
 
-Memory: checkpoints take ceil(N/K) x 3 planes per transmitter, the segment
-buffer K+1 x 3 planes, shared by all transmitters.
+Memory: checkpoints take ceil(N/K) x 3 planes per transmitter; the reverse
+pass runs transmitters in groups whose segment buffers ((K+1) x 3 planes each)
+fit 2 GB, one launch per step for the whole group.
 """
 
 from __future__ import annotations
@@ -133,31 +134,64 @@ class MisfitProblem2D:
         return traces, ckpt
 
     def adjoint(self, ca, cb, ckpt, resid):
-        """float64 dL/dCa, dL/dCb summed over the transmitters."""
+        """float64 dL/dCa, dL/dCb summed over the transmitters: (n_tx, Nx*Ny)
+        accumulator planes, one per transmitter."""
         g, dev, N, K = self.grid, self.device, self.n_steps, self.K
-        lib = nat.load()
-        stream = nat.stream_handle(dev)
-        gca = torch.zeros((g.Nx, g.Ny), dtype=torch.float64, device=dev)
+        cells = g.Nx * g.Ny
+        gca = torch.zeros((len(self.sources), cells), dtype=torch.float64, device=dev)
         gcb = torch.zeros_like(gca)
-        states = torch.empty((min(K, N) + 1, 3, g.Nx, g.Ny), dtype=torch.float32, device=dev)
-        lam = torch.empty((3, g.Nx, g.Ny), dtype=torch.float32, device=dev)
-        lam_s = torch.empty_like(lam)
-        for t, st in enumerate(self.sources):
-            lam.zero_()
-            r = resid[t]
-            for s in reversed(range(self.n_segments)):
-                s0 = s * K
-                ns = min(K, N - s0)
-                states[0].copy_(ckpt[t, s])
-                nat.check(lib.wf_fdtd2d_states(ctypes.byref(self.g), states.data_ptr(), ns,
-                                               ca.data_ptr(), cb.data_ptr(), st.ptr, st.count, s0,
-                                               stream))
-                nat.check(lib.wf_adjoint2d_run(ctypes.byref(self.g), states.data_ptr(), ns,
-                                               ca.data_ptr(), cb.data_ptr(), self.probes.ptr,
-                                               self.probes.count, r.data_ptr(), r.stride(0), 0,
-                                               s0, lam.data_ptr(), lam_s.data_ptr(),
-                                               gca.data_ptr(), gcb.data_ptr(), stream))
+        adjoint_runs(self.g, cells, N, K, ca, cb, ckpt, resid, self.sources, self.probes,
+                     gca, gcb, dev)
         return gca, gcb
+
+
+def tx_group(n_tx: int, K: int, cells: int, budget: float = 2e9) -> int:
+    """Transmitter runs whose segment buffers ((K+1) x 3 planes each) fit
+    ``budget`` bytes, at least one."""
+    return max(1, min(n_tx, int(budget // ((K + 1) * 3 * cells * 4))))
+
+
+def adjoint_runs(g, cells: int, N: int, K: int, ca, cb, ckpt, resid, sources, probes,
+                 gca, gcb, dev, stream=None, keep: Optional[list] = None) -> None:
+    """Reverse pass of every transmitter run: for each group of runs and each
+    checkpoint segment from last to first, recompute the segment's states
+    (wf_fdtd2d_states) and run the adjoint steps (wf_adjoint2d_run), one
+    launch per step for the whole group.  ``sources``: one SourceTable per
+    run; ``ckpt``: (n_tx, n_seg, 3, cells); ``resid``: (n_tx, n_rx, N);
+    ``gca``/``gcb``: (n_tx, cells) float64 accumulators."""
+    lib = nat.load()
+    st = nat.stream_handle(dev) if stream is None else stream
+    n_tx = len(sources)
+    nseg = -(-N // K)
+    counts = {s.count for s in sources}
+    G = tx_group(n_tx, min(K, N), cells) if len(counts) == 1 else 1
+    states = torch.empty((G, min(K, N) + 1, 3, cells), dtype=torch.float32, device=dev)
+    lam = torch.empty((G, 3, cells), dtype=torch.float32, device=dev)
+    lam_s = torch.empty_like(lam)
+    if keep is not None:
+        keep.extend([states, lam, lam_s])
+    for t0 in range(0, n_tx, G):
+        grp = sources[t0:t0 + G]
+        ng = len(grp)
+        srcs = [s.dev for s in grp if s.dev is not None]
+        src = torch.cat(srcs) if srcs else None
+        if keep is not None and src is not None:
+            keep.append(src)
+        per = grp[0].count
+        lam[:ng].zero_()
+        for s in reversed(range(nseg)):
+            s0 = s * K
+            ns = min(K, N - s0)
+            states[:ng, 0].copy_(ckpt[t0:t0 + ng, s].reshape(ng, 3, cells))
+            nat.check(lib.wf_fdtd2d_states(ctypes.byref(g), states.data_ptr(), states.stride(0), ng,
+                                           ns, ca.data_ptr(), cb.data_ptr(),
+                                           None if src is None else src.data_ptr(), per, s0, st))
+            nat.check(lib.wf_adjoint2d_run(ctypes.byref(g), states.data_ptr(), states.stride(0), ng,
+                                           ns, ca.data_ptr(), cb.data_ptr(), probes.ptr,
+                                           probes.count, resid[t0].data_ptr(), resid.stride(1),
+                                           resid.stride(0), 0, s0, lam.data_ptr(),
+                                           lam_s.data_ptr(), gca[t0].data_ptr(),
+                                           gcb[t0].data_ptr(), st))
 
 
 def _plane64(x: torch.Tensor, g: YeeGrid, device, what: str) -> torch.Tensor:
@@ -200,8 +234,8 @@ class FDTDMisfit(torch.autograd.Function):
         geps = torch.empty_like(e64)
         gsig = torch.empty_like(s64)
         nat.check(nat.load().wf_material_grad(e64.data_ptr(), s64.data_ptr(), e64.numel(),
-                                              problem.grid.dt, gca.data_ptr(), gcb.data_ptr(), 1.0,
-                                              geps.data_ptr(), gsig.data_ptr(),
+                                              problem.grid.dt, gca.data_ptr(), gcb.data_ptr(),
+                                              gca.shape[0], 1.0, geps.data_ptr(), gsig.data_ptr(),
                                               nat.stream_handle(problem.device)))
         scale = grad_out.to(torch.float64)
         eshape, edtype, sshape, sdtype = ctx.shapes

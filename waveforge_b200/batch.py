@@ -21,6 +21,7 @@ import ctypes
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
+import numpy as np
 import torch
 
 from . import _native as nat
@@ -62,11 +63,92 @@ def grid_struct(grid: YeeGrid, device: Optional[torch.device] = None) -> nat.WfG
                         nat.f32(grid.dy), nat.f32(cm[0]), nat.f32(cm[1]), flags)
 
 
+
+class PassPlan:
+    """Pass schedule of a temporally blocked run (the plan of wf_common.cuh
+    PassPlan): ``nsteps`` split into passes of at most ``K`` steps, the first
+    pass split in two when the pass count is odd so the ping-pong ends in the
+    state buffers; only an odd run of single-step passes needs a copy-back."""
+
+    def __init__(self, nsteps: int, K: int) -> None:
+        self.nsteps, self.K = nsteps, K
+        self.P0 = -(-nsteps // K)
+        L0 = min(nsteps, K)
+        self.split = 1 if (self.P0 % 2 == 1 and L0 >= 2) else 0
+        self.a = L0 // 2
+
+    @property
+    def passes(self) -> int:
+        return self.P0 + self.split
+
+    def _unsplit(self, q: int) -> int:
+        return self.K if q < self.P0 - 1 else self.nsteps - self.K * (self.P0 - 1)
+
+    def length(self, p: int) -> int:
+        if not self.split:
+            return self._unsplit(p)
+        if p == 0:
+            return self.a
+        if p == 1:
+            return self._unsplit(0) - self.a
+        return self._unsplit(p - 1)
+
+    def offset(self, p: int) -> int:
+        if not self.split:
+            return p * self.K
+        if p == 0:
+            return 0
+        if p == 1:
+            return self.a
+        return (p - 1) * self.K
+
+    @property
+    def needs_copy(self) -> bool:
+        return self.passes % 2 == 1
+
+
+def tile_items(shapes: Sequence[tuple[int, int]], k: int, region: tuple[int, int],
+               index: Optional[Sequence[int]] = None) -> np.ndarray:
+    """(solve index, ci0, cj0) int32 triplets of every core tile of every
+    solve for a pass of ``k`` steps with an RH x RW region (core RH-2k x
+    RW-2k), largest solves first."""
+    rh, rw = region
+    ci, cj = rh - 2 * k, rw - 2 * k
+    out = []
+    idx = list(range(len(shapes))) if index is None else list(index)
+    for q, (nx, ny) in sorted(zip(idx, shapes), key=lambda t: -t[1][0] * t[1][1]):
+        ii, jj = np.meshgrid(np.arange(0, nx, ci, dtype=np.int32),
+                             np.arange(0, ny, cj, dtype=np.int32), indexing="ij")
+        t = np.empty((ii.size, 3), dtype=np.int32)
+        t[:, 0] = q
+        t[:, 1] = ii.reshape(-1)
+        t[:, 2] = jj.reshape(-1)
+        out.append(t)
+    return np.concatenate(out) if out else np.zeros((0, 3), dtype=np.int32)
+
+
+def run_tiled_passes(desc_dev_ptr: int, items_by_k: dict, plan: PassPlan, tune, fastdiv: bool,
+                     stream: int) -> None:
+    """Launch every pass of ``plan`` as one wf_batch2d_pass over its items
+    (``items_by_k[k]`` = (device pointer, count))."""
+    lib = nat.load()
+    for p in range(plan.passes):
+        k = plan.length(p)
+        ptr, n = items_by_k[k]
+        nat.check(lib.wf_batch2d_pass(desc_dev_ptr, ptr, n, p & 1, plan.offset(p), k,
+                                      None if tune is None else ctypes.byref(tune),
+                                      1 if fastdiv else 0, stream))
+
+
 class Batch2D:
     """Device-resident set of solves advanced by one persistent launch per call."""
 
     def __init__(self, solves: Sequence[BatchSolve], n_steps: int, *, tune=None,
-                 ctas_per_sm: int = 0, device=None) -> None:
+                 ctas_per_sm: int = 0, device=None, mode: str = "persistent") -> None:
+        if mode not in ("persistent", "tiled"):
+            raise ValueError("mode is 'persistent' (one CTA per solve, one launch) or 'tiled' "
+                             "(one launch per pass over every solve's tiles)")
+        self.mode = mode
         if not solves:
             raise ValueError("Batch2D needs at least one solve")
         self.device = torch.device(device) if device is not None else solves[0].grid.device
@@ -145,6 +227,7 @@ class Batch2D:
         return self._offs[-1]
 
     def _upload(self, step0: int, nsteps: int) -> None:
+        self._launch_nsteps = nsteps
         for d in self._desc:
             d.step0 = step0
             d.nsteps = nsteps
@@ -166,8 +249,43 @@ class Batch2D:
         self.launch()
         self.step += nsteps
 
+    @property
+    def region(self) -> tuple[int, int]:
+        t = self.tune
+        return (48, 128) if t is None else (t.tile_i, t.tile_j)
+
+    @property
+    def depth(self) -> int:
+        return 6 if self.tune is None else self.tune.steps_per_pass
+
+    def launches_per_run(self) -> int:
+        """Kernel launches of one full ``run()``."""
+        if self.mode == "persistent":
+            return 1
+        plan = PassPlan(self.n_steps, self.depth)
+        return plan.passes
+
+    def _items(self, k: int):
+        cache = self.__dict__.setdefault("_item_cache", {})
+        if k not in cache:
+            shapes = [(s.grid.Nx, s.grid.Ny) for s in self.solves]
+            it = torch.from_numpy(tile_items(shapes, k, self.region)).to(self.device)
+            cache[k] = (it, it.shape[0])
+        t, n = cache[k]
+        return t.data_ptr(), n
+
     def launch(self) -> None:
-        """Queue reset + the persistent launch (capturable in a CUDA graph)."""
+        """Advance every solve by the uploaded step count: one persistent
+        launch ("persistent"), or one tile-queue launch per temporal pass
+        ("tiled"); either sequence can be captured in a CUDA graph."""
+        if self.mode == "tiled":
+            plan = PassPlan(self._launch_nsteps, self.depth)
+            items = {plan.length(p): self._items(plan.length(p)) for p in range(plan.passes)}
+            run_tiled_passes(self._desc_dev.data_ptr(), items, plan, self.tune, self._fastdiv,
+                             nat.stream_handle(self.device))
+            if plan.needs_copy:
+                self._state.copy_(self._scratch)
+            return
         self._queue.zero_()
         lib = nat.load()
         nat.check(lib.wf_batch2d_run(self._desc_dev.data_ptr(), len(self.solves),

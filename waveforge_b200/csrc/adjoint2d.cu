@@ -25,8 +25,12 @@
 //
 // k_adj2d_step: one CTA produces a TI x TJ tile of lambda_n from a region of
 // lambda_{n+1} with a 3-cell halo staged in shared memory; the chain
-// aHy -> aHx -> aHc needs radius 3.  Gradient accumulators are float64 (one
-// read-modify-write per cell and step by its owning thread).
+// aHy -> aHx -> aHc needs radius 3.  blockIdx.y selects one of several
+// transmitter runs that share the grid and coefficients, so one launch per
+// reverse step covers all of them.  Gradient accumulators are float64, one
+// plane pair per run (one read-modify-write per cell and step by its owning
+// thread); wf_material_grad sums them in run order, so the result does not
+// depend on how runs are grouped into launches.
 #include "wf_common.cuh"
 
 namespace wf {
@@ -49,6 +53,9 @@ struct Adj2D {
   long long resid_ld;
   int col;
   double *gca, *gcb;                 // accumulated dL/dCa, dL/dCb (MAT only)
+  // per-run strides (blockIdx.y = run): states, adjoint planes, residual rows,
+  // accumulator planes
+  long long st_stride, lam_stride, resid_stride, g_stride;
 };
 
 template <bool MAT>
@@ -59,6 +66,22 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj2d_step(Adj2D A, int tiles_j
   __shared__ float sB[kAdjRI][kAdjRJ];   // Cb (or De), later aHc
   __shared__ float sY[kAdjRI][kAdjRJ];   // aHy
   const int nx = A.nx, ny = A.ny;
+  {
+    // this CTA's transmitter run
+    const long long r = blockIdx.y;
+    A.ex_n += r * A.st_stride;
+    A.ey_n += r * A.st_stride;
+    A.hz_n1 += r * A.st_stride;
+    for (int c = 0; c < 3; ++c) {
+      A.lin[c] += r * A.lam_stride;
+      A.lout[c] += r * A.lam_stride;
+    }
+    A.resid += r * A.resid_stride;
+    if (MAT) {
+      A.gca += r * A.g_stride;
+      A.gcb += r * A.g_stride;
+    }
+  }
   const int bi = blockIdx.x / tiles_j, bj = blockIdx.x - bi * tiles_j;
   const int i0 = bi * kAdjTI - kAdjHalo, j0 = bj * kAdjTJ - kAdjHalo;  // region origin
   const int tid = threadIdx.x;
@@ -220,10 +243,16 @@ __global__ void k_material_coeffs(const double* __restrict__ eps, const double* 
 //   dCb/dsigma = -(dt/eps0) / D^2 * dt / (2 eps0).
 __global__ void k_material_grad(const double* __restrict__ eps, const double* __restrict__ sig,
                                 long long n, double dt, const double* __restrict__ gca,
-                                const double* __restrict__ gcb, double scale,
+                                const double* __restrict__ gcb, int count, double scale,
                                 double* __restrict__ geps, double* __restrict__ gsig) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
        q += (long long)gridDim.x * blockDim.x) {
+    // sum of the per-run accumulators, always in run order
+    double ga = gca[q], gb = gcb[q];
+    for (int c = 1; c < count; ++c) {
+      ga += gca[c * n + q];
+      gb += gcb[c * n + q];
+    }
     const double e = eps[q], s = sig[q];
     const double k = dt / (2.0 * kEps0);
     const double alpha = s * k / e;
@@ -231,8 +260,8 @@ __global__ void k_material_grad(const double* __restrict__ eps, const double* __
     const double dca_da = -2.0 / (opa * opa);
     const double D = e + s * k;
     const double dcb_dD = -(dt / kEps0) / (D * D);
-    geps[q] = scale * (gca[q] * dca_da * (-alpha / e) + gcb[q] * dcb_dD);
-    gsig[q] = scale * (gca[q] * dca_da * (k / e) + gcb[q] * dcb_dD * k);
+    geps[q] = scale * (ga * dca_da * (-alpha / e) + gb * dcb_dD);
+    gsig[q] = scale * (ga * dca_da * (k / e) + gb * dcb_dD * k);
   }
 }
 
@@ -240,12 +269,12 @@ __global__ void k_material_grad(const double* __restrict__ eps, const double* __
 
 using namespace wf;
 
-extern "C" int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int32_t nsteps,
-                                    const float* ca, const float* cb, const wf_probe* probes,
-                                    int32_t nprobe, const float* resid, int64_t resid_ld,
-                                    int32_t resid_step0, int32_t step0, float* lam,
-                                    float* lam_scratch, double* g_ca, double* g_cb,
-                                    void* stream) {
+extern "C" int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int64_t states_stride,
+                                    int32_t ntx, int32_t nsteps, const float* ca, const float* cb,
+                                    const wf_probe* probes, int32_t nprobe, const float* resid,
+                                    int64_t resid_ld, int64_t resid_stride, int32_t resid_step0,
+                                    int32_t step0, float* lam, float* lam_scratch, double* g_ca,
+                                    double* g_cb, void* stream) {
   if (g == nullptr || states == nullptr || lam == nullptr || lam_scratch == nullptr)
     return set_error(WF_E_ARG, "wf_adjoint2d_run: null grid/states/adjoint pointer");
   if (g->nx < 4 || g->ny < 4)
@@ -255,14 +284,16 @@ extern "C" int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int
     return set_error(WF_E_ARG, "wf_adjoint2d_run: Ca and Cb must be given together");
   if (ca != nullptr && (g_ca == nullptr || g_cb == nullptr))
     return set_error(WF_E_ARG, "wf_adjoint2d_run: gradient accumulators required with Ca/Cb");
-  if (nsteps < 0 || step0 < 0 || nprobe < 0 || (nprobe > 0 && (probes == nullptr || resid == nullptr)))
-    return set_error(WF_E_ARG, "wf_adjoint2d_run: bad counts or null probe/residual arrays");
+  const long long cells = (long long)g->nx * g->ny;
+  if (nsteps < 0 || step0 < 0 || nprobe < 0 || ntx < 1 || ntx > 65535 ||
+      (nprobe > 0 && (probes == nullptr || resid == nullptr)) ||
+      (ntx > 1 && states_stride < (long long)(nsteps + 1) * 3 * cells))
+    return set_error(WF_E_ARG, "wf_adjoint2d_run: bad counts, stride or null probe/residual arrays");
   if (nprobe > 0 && step0 < resid_step0)
     return set_error(WF_E_ARG, "wf_adjoint2d_run: step0 %d precedes the residual's first step %d",
                      step0, resid_step0);
   if (nsteps == 0) return WF_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  const long long cells = (long long)g->nx * g->ny;
   Adj2D A{};
   A.nx = g->nx;
   A.ny = g->ny;
@@ -280,6 +311,10 @@ extern "C" int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int
   A.resid_ld = resid_ld;
   A.gca = g_ca;
   A.gcb = g_cb;
+  A.st_stride = states_stride;
+  A.lam_stride = 3 * cells;
+  A.resid_stride = resid_stride;
+  A.g_stride = cells;
   const int tiles_i = (g->nx + kAdjTI - 1) / kAdjTI, tiles_j = (g->ny + kAdjTJ - 1) / kAdjTJ;
   float* L[2] = {lam, lam_scratch};
   for (int t = nsteps - 1, p = 0; t >= 0; --t, ++p) {
@@ -295,13 +330,14 @@ extern "C" int32_t wf_adjoint2d_run(const wf_grid2d* g, const float* states, int
       A.lout[c] = out + c * cells;
     }
     A.col = step0 + t - resid_step0;
-    if (ca) k_adj2d_step<true><<<tiles_i * tiles_j, kAdjThreads, 0, st>>>(A, tiles_j);
-    else k_adj2d_step<false><<<tiles_i * tiles_j, kAdjThreads, 0, st>>>(A, tiles_j);
+    dim3 grid(tiles_i * tiles_j, ntx);
+    if (ca) k_adj2d_step<true><<<grid, kAdjThreads, 0, st>>>(A, tiles_j);
+    else k_adj2d_step<false><<<grid, kAdjThreads, 0, st>>>(A, tiles_j);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "launch k_adj2d_step");
   }
   if (nsteps & 1) {
-    k_copy3f<<<296, 256, 0, st>>>(lam_scratch, lam, 3 * cells);
+    k_copy3f<<<296, 256, 0, st>>>(lam_scratch, lam, 3 * cells * ntx);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "launch k_copy3f");
   }
@@ -322,14 +358,15 @@ extern "C" int32_t wf_material_coeffs(const double* eps_r, const double* sigma, 
 
 extern "C" int32_t wf_material_grad(const double* eps_r, const double* sigma, int64_t n,
                                     double dt, const double* g_ca, const double* g_cb,
-                                    double scale, double* g_eps, double* g_sigma, void* stream) {
-  if (n < 0 || (n > 0 && (eps_r == nullptr || sigma == nullptr || g_ca == nullptr ||
-                          g_cb == nullptr || g_eps == nullptr || g_sigma == nullptr)))
-    return set_error(WF_E_ARG, "wf_material_grad: null pointer or negative size");
+                                    int32_t count, double scale, double* g_eps, double* g_sigma,
+                                    void* stream) {
+  if (n < 0 || count < 1 || (n > 0 && (eps_r == nullptr || sigma == nullptr || g_ca == nullptr ||
+                                       g_cb == nullptr || g_eps == nullptr || g_sigma == nullptr)))
+    return set_error(WF_E_ARG, "wf_material_grad: null pointer, negative size or count < 1");
   if (!(dt > 0.0)) return set_error(WF_E_ARG, "wf_material_grad: dt must be positive");
   if (n == 0) return WF_OK;
-  k_material_grad<<<592, 256, 0, (cudaStream_t)stream>>>(eps_r, sigma, n, dt, g_ca, g_cb, scale,
-                                                         g_eps, g_sigma);
+  k_material_grad<<<592, 256, 0, (cudaStream_t)stream>>>(eps_r, sigma, n, dt, g_ca, g_cb, count,
+                                                         scale, g_eps, g_sigma);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "launch k_material_grad");
   return WF_OK;

@@ -134,6 +134,89 @@ struct LaunchBatch {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Tile-queue form: one launch = one temporal pass of every listed solve.
+// Work items are (solve, tile origin) triplets; each CTA takes one item and
+// runs the same tile routine as the plain kernel on it, so every solve's
+// result is bit-identical to its plain run, while a large grid's tiles spread
+// over all SMs instead of one.  All solves of one pass sequence advance the
+// same number of steps from their own step0; pass p reads the state buffers
+// when `parity` is 0 and the scratch buffers when it is 1, and writes the other.
+// ---------------------------------------------------------------------------
+template <class C, bool FDIV>
+__global__ void __launch_bounds__(C::THREADS, 1) k_batch_pass(const wf_solve2d* __restrict__ solves,
+                                                              const int* __restrict__ items,
+                                                              int parity, int s_off, int k) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TileSmem<C>& sm = *reinterpret_cast<TileSmem<C>*>(smraw);
+  const int* it = items + 3 * (long long)blockIdx.x;
+  const wf_solve2d& S = solves[it[0]];
+  const int ci0 = it[1], cj0 = it[2];
+  Tile2D P{};
+  P.nx = S.g.nx;
+  P.ny = S.g.ny;
+  P.dh = S.g.dh;
+  P.de = S.g.de;
+  P.dx = S.g.dx;
+  P.dy = S.g.dy;
+  P.mx = S.g.mur_x;
+  P.my = S.g.mur_y;
+  P.fastdiv = S.g.flags;
+  P.ca = S.ca;
+  P.cb = S.cb;
+  P.src = S.src;
+  P.nsrc = S.nsrc;
+  P.prb = S.probes;
+  P.nprb = S.nprobe;
+  P.traces = S.traces;
+  P.trace_ld = S.trace_ld;
+  P.trace_step0 = S.trace_step0;
+  P.n_check = S.n_check;
+  P.check_max = S.check_max;
+  P.check_base = S.n_check > 0 ? S.step0 / S.n_check : 0;
+  P.status = nullptr;
+  const float* A[3] = {S.ex, S.ey, S.hz};
+  const float* B[3] = {S.sx, S.sy, S.sz};
+  P.ex_in = parity ? B[0] : A[0];
+  P.ey_in = parity ? B[1] : A[1];
+  P.hz_in = parity ? B[2] : A[2];
+  P.ex_out = const_cast<float*>(parity ? A[0] : B[0]);
+  P.ey_out = const_cast<float*>(parity ? A[1] : B[1]);
+  P.hz_out = const_cast<float*>(parity ? A[2] : B[2]);
+  const int ci = C::RH - 2 * k, cj = C::RW - 2 * k;
+  const int ci1 = min(ci0 + ci, P.nx), cj1 = min(cj0 + cj, P.ny);
+  const int s0 = S.step0 + s_off;
+  if (S.ca != nullptr) tile2d<C, true, FDIV>(P, ci0, ci1, cj0, cj1, s0, k, sm);
+  else tile2d<C, false, FDIV>(P, ci0, ci1, cj0, cj1, s0, k, sm);
+}
+
+struct LaunchPassBatch {
+  const wf_solve2d* solves;
+  const int* items;
+  int nitems, parity, s_off, k;
+  bool fdiv;
+  cudaStream_t st;
+  template <class C>
+  int operator()() const {
+    return fdiv ? go<C, true>() : go<C, false>();
+  }
+  template <class C, bool FDIV>
+  int go() const {
+    const size_t smem = sizeof(TileSmem<C>);
+    static bool attr_done = false;
+    if (!attr_done) {
+      cudaError_t e = cudaFuncSetAttribute(k_batch_pass<C, FDIV>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_batch_pass)");
+      attr_done = true;
+    }
+    k_batch_pass<C, FDIV><<<nitems, C::THREADS, smem, st>>>(solves, items, parity, s_off, k);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "launch k_batch_pass");
+    return WF_OK;
+  }
+};
+
 }  // namespace wf
 
 using namespace wf;
@@ -160,4 +243,26 @@ extern "C" int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve, cons
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
   return dispatch_cfg2d(t, LaunchBatch{solves, order, nsolve, queue, t.steps_per_pass,
                                        ctas_per_sm, nsm, fastdiv != 0, (cudaStream_t)stream});
+}
+
+extern "C" int32_t wf_batch2d_pass(const wf_solve2d* solves, const int32_t* items,
+                                   int32_t nitems, int32_t parity, int32_t step_offset,
+                                   int32_t k, const wf_tune* tune, int32_t fastdiv,
+                                   void* stream) {
+  if (nitems < 0 || (nitems > 0 && (solves == nullptr || items == nullptr)))
+    return set_error(WF_E_ARG, "wf_batch2d_pass: null descriptor/item pointer");
+  if (nitems == 0) return WF_OK;
+  if (parity != 0 && parity != 1) return set_error(WF_E_ARG, "wf_batch2d_pass: parity is 0 or 1");
+  if (step_offset < 0) return set_error(WF_E_ARG, "wf_batch2d_pass: negative step offset");
+  wf_tune t{};
+  if (tune) {
+    t = *tune;
+  } else {
+    t.tile_i = 48;
+    t.tile_j = 128;
+  }
+  t.steps_per_pass = k;
+  if (int rc = check_tune2d(t)) return rc;
+  return dispatch_cfg2d(t, LaunchPassBatch{solves, items, nitems, parity, step_offset, k,
+                                           fastdiv != 0, (cudaStream_t)stream});
 }

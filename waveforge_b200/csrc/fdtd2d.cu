@@ -23,6 +23,29 @@ __global__ void __launch_bounds__(C::THREADS, 1) k2d_pass(Tile2D P, int ci, int 
   tile2d<C, MAT, FDIV>(P, ci0, min(ci0 + ci, P.nx), cj0, min(cj0 + cj, P.ny), step0, k, S);
 }
 
+// One single-step pass for each of gridDim.y transmitter runs that share the
+// grid and coefficients: run t reads slot P.*_in + t*tx_stride, writes the
+// matching output slot, and uses sources [t*src_per_tx, (t+1)*src_per_tx).
+template <class C, bool MAT, bool FDIV>
+__global__ void __launch_bounds__(C::THREADS, 1) k2d_states_tx(Tile2D P, int ci, int cj,
+                                                               int tiles_j, int step0,
+                                                               long long tx_stride,
+                                                               int src_per_tx) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TileSmem<C>& S = *reinterpret_cast<TileSmem<C>*>(smraw);
+  const long long o = blockIdx.y * tx_stride;
+  P.ex_in += o;
+  P.ey_in += o;
+  P.hz_in += o;
+  P.ex_out += o;
+  P.ey_out += o;
+  P.hz_out += o;
+  P.src += blockIdx.y * src_per_tx;
+  const int bi = blockIdx.x / tiles_j, bj = blockIdx.x - bi * tiles_j;
+  const int ci0 = bi * ci, cj0 = bj * cj;
+  tile2d<C, MAT, FDIV>(P, ci0, min(ci0 + ci, P.nx), cj0, min(cj0 + cj, P.ny), step0, 1, S);
+}
+
 __global__ void k_copy3(const float* __restrict__ a, const float* __restrict__ b,
                         const float* __restrict__ c, float* __restrict__ x,
                         float* __restrict__ y, float* __restrict__ z, long long n) {
@@ -81,6 +104,45 @@ struct LaunchPass {
                          : launch_pass_cfg<C, true, false>(P, k, step0, st);
     return fdiv ? launch_pass_cfg<C, false, true>(P, k, step0, st)
                 : launch_pass_cfg<C, false, false>(P, k, step0, st);
+  }
+};
+
+template <class C, bool MAT, bool FDIV>
+static int launch_states_cfg(const Tile2D& P, int step0, int ntx, long long tx_stride,
+                             int src_per_tx, cudaStream_t st) {
+  const int ci = C::RH - 2, cj = C::RW - 2;
+  const int tiles_i = (P.nx + ci - 1) / ci, tiles_j = (P.ny + cj - 1) / cj;
+  const size_t smem = sizeof(TileSmem<C>);
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k2d_states_tx<C, MAT, FDIV>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k2d_states_tx)");
+    attr_done = true;
+  }
+  const long long nblk = (long long)tiles_i * tiles_j;
+  if (nblk > 0x7fffffffLL || ntx > 65535) return set_error(WF_E_LIMIT, "wf_fdtd2d_states: grid too large");
+  dim3 grid((unsigned)nblk, (unsigned)ntx);
+  k2d_states_tx<C, MAT, FDIV><<<grid, C::THREADS, smem, st>>>(P, ci, cj, tiles_j, step0, tx_stride,
+                                                              src_per_tx);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "launch k2d_states_tx");
+  return WF_OK;
+}
+
+struct LaunchStates {
+  const Tile2D& P;
+  int step0, ntx;
+  long long tx_stride;
+  int src_per_tx;
+  cudaStream_t st;
+  bool mat, fdiv;
+  template <class C>
+  int operator()() const {
+    if (mat) return fdiv ? launch_states_cfg<C, true, true>(P, step0, ntx, tx_stride, src_per_tx, st)
+                         : launch_states_cfg<C, true, false>(P, step0, ntx, tx_stride, src_per_tx, st);
+    return fdiv ? launch_states_cfg<C, false, true>(P, step0, ntx, tx_stride, src_per_tx, st)
+                : launch_states_cfg<C, false, false>(P, step0, ntx, tx_stride, src_per_tx, st);
   }
 };
 
@@ -163,9 +225,10 @@ extern "C" int32_t wf_fdtd2d_run(const wf_grid2d* g, float* ex, float* ey, float
   return WF_OK;
 }
 
-extern "C" int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int32_t nsteps,
-                                    const float* ca, const float* cb, const wf_source* src,
-                                    int32_t nsrc, int32_t step0, void* stream) {
+extern "C" int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int64_t tx_stride,
+                                    int32_t ntx, int32_t nsteps, const float* ca, const float* cb,
+                                    const wf_source* src, int32_t src_per_tx, int32_t step0,
+                                    void* stream) {
   if (g == nullptr || states == nullptr)
     return set_error(WF_E_ARG, "wf_fdtd2d_states: null grid/states pointer");
   if (g->nx < 4 || g->ny < 4)
@@ -173,9 +236,12 @@ extern "C" int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int32_t n
                      g->nx, g->ny);
   if ((ca == nullptr) != (cb == nullptr))
     return set_error(WF_E_ARG, "wf_fdtd2d_states: Ca and Cb must be given together");
-  if (nsteps < 0 || step0 < 0 || nsrc < 0 || (nsrc > 0 && src == nullptr))
-    return set_error(WF_E_ARG, "wf_fdtd2d_states: bad counts or null source array");
-  if (nsrc > 32767) return set_error(WF_E_LIMIT, "wf_fdtd2d_states: at most 32767 sources");
+  const long long cells = (long long)g->nx * g->ny;
+  if (nsteps < 0 || step0 < 0 || src_per_tx < 0 || ntx < 1 ||
+      (src_per_tx > 0 && src == nullptr) ||
+      (ntx > 1 && tx_stride < (long long)(nsteps + 1) * 3 * cells))
+    return set_error(WF_E_ARG, "wf_fdtd2d_states: bad counts, stride or null source array");
+  if (src_per_tx > 32767) return set_error(WF_E_LIMIT, "wf_fdtd2d_states: at most 32767 sources");
   if (nsteps == 0) return WF_OK;
   wf_tune t = default_tune2d(g->nx, g->ny);
   t.steps_per_pass = 1;
@@ -194,9 +260,8 @@ extern "C" int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int32_t n
   P.ca = ca;
   P.cb = cb;
   P.src = src;
-  P.nsrc = nsrc;
+  P.nsrc = src_per_tx;
   const bool fdiv = (g->flags & (WF_FASTDIV_X | WF_FASTDIV_Y)) == (WF_FASTDIV_X | WF_FASTDIV_Y);
-  const long long cells = (long long)g->nx * g->ny;
   for (int s = 0; s < nsteps; ++s) {
     float* in = states + (long long)s * 3 * cells;
     float* out = in + 3 * cells;
@@ -206,7 +271,8 @@ extern "C" int32_t wf_fdtd2d_states(const wf_grid2d* g, float* states, int32_t n
     P.ex_out = out;
     P.ey_out = out + cells;
     P.hz_out = out + 2 * cells;
-    const int rc = dispatch_cfg2d(t, LaunchPass{P, 1, step0 + s, st, ca != nullptr, fdiv});
+    const int rc = dispatch_cfg2d(t, LaunchStates{P, step0 + s, ntx, tx_stride, src_per_tx, st,
+                                                  ca != nullptr, fdiv});
     if (rc) return rc;
   }
   return WF_OK;

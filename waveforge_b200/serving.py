@@ -5,8 +5,11 @@ transmitter, one after another (examples/brain_mimo_imaging.py:149-204), and
 its dataset generator does the same per sample (src/datasets/generator.py:
 162-248).  ``Server`` keeps every admitted request's fields, coefficients,
 traces (and, for gradient requests, checkpoints) resident on the device and
-advances ALL admitted solves together, one chunk of ``chunk_steps`` steps per
-persistent ``wf_batch2d_run`` launch.  Between chunks it
+advances ALL admitted solves together by one chunk of ``chunk_steps`` steps
+at a time: in the default "tiled" mode each temporal pass of the chunk is one
+``wf_batch2d_pass`` launch over the tiles of every admitted solve (a large
+grid spreads over all SMs); the "persistent" mode runs the chunk as one
+``wf_batch2d_run`` launch with one CTA per solve.  Between chunks it
 
 * admits queued requests in arrival order while their HBM footprint fits the
   budget (their phantoms are painted on the device by ``wf_paint2d``; only
@@ -32,10 +35,11 @@ import time
 from dataclasses import dataclass
 from typing import Optional, Sequence
 
+import numpy as np
 import torch
 
 from . import _native as nat
-from .batch import grid_struct
+from .batch import PassPlan, grid_struct, run_tiled_passes, tile_items
 from .core._engine import ProbeTable
 from .core.materials import MaterialMap
 
@@ -101,11 +105,22 @@ def request_footprint(req: ImagingRequest, chunk: int) -> int:
     b += nsol * nrx * req.n_steps * 4              # traces
     if grad:
         nseg = -(-req.n_steps // chunk)
+        from .adjoint import tx_group
+        G = tx_group(ntx, min(chunk, req.n_steps), cells)
         b += ntx * nseg * 3 * cells * 4            # checkpoints
-        b += (chunk + 1) * 3 * cells * 4 + 2 * 3 * cells * 4   # segment states, adjoint
-        b += 6 * cells * 8                         # eps, sigma, dL/dCa, dL/dCb, grads
+        b += G * (min(chunk, req.n_steps) + 1 + 2) * 3 * cells * 4   # segment states, adjoint
+        b += 2 * ntx * cells * 8 + 4 * cells * 8   # dL/dCa, dL/dCb per run; eps, sigma, grads
         b += ntx * nrx * req.n_steps * 4           # residual
     return b
+
+
+class _SrcView:
+    """One transmitter's single source inside a request's source array (the
+    SourceTable interface the adjoint driver reads: dev, count)."""
+
+    def __init__(self, table: torch.Tensor, offset: int) -> None:
+        self.dev = table[offset:offset + ctypes.sizeof(nat.WfSource)]
+        self.count = 1
 
 
 class _Live:
@@ -180,16 +195,34 @@ class _Live:
             d.n_check = 0
             d.check_max = None
             self.desc.append(d)
+        # descriptor bytes of the request's solves, patched per chunk (step0,
+        # nsteps, status) through an int32 view
+        self.desc_np = np.frombuffer(bytearray(bytes(memoryview(
+            (nat.WfSolve2D * self.nsol)(*self.desc)).cast("B"))), dtype=np.uint8).copy()
+        self.items: dict = {}   # k -> (solve-local index, ci0, cj0) int32 rows
         self.event = None
         self.host_traces = None
+
+    def tile_rows(self, k: int, region: tuple[int, int]) -> np.ndarray:
+        if k not in self.items:
+            self.items[k] = tile_items([(self.nx, self.ny)] * self.nsol, k, region)
+        return self.items[k]
 
 
 class Server:
     """Continuous-batching server on one device (see the module docstring)."""
 
-    def __init__(self, device, *, hbm_budget: float = 60e9, chunk_steps: int = 64,
+    def __init__(self, device, *, hbm_budget: float = 60e9, chunk_steps: int = 128,
                  max_wait_s: Optional[float] = None, max_active_solves: Optional[int] = None,
-                 tune=None, ctas_per_sm: int = 0) -> None:
+                 max_active_cells: float = 3.2e7, mode: str = "tiled", tune=None,
+                 ctas_per_sm: int = 0) -> None:
+        if mode not in ("tiled", "persistent"):
+            raise ValueError("mode is 'tiled' or 'persistent'")
+        self.mode = mode
+        # tiled: a pass spreads every solve's tiles over all SMs, so a few
+        # requests already fill the GPU; the in-flight cell cap bounds how
+        # many requests share it (and so each one's latency)
+        self.max_cells = int(max_active_cells)
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("Server runs on a CUDA device only (no CPU fallback)")
@@ -204,6 +237,8 @@ class Server:
         self.chunk = int(chunk_steps)
         self.max_wait_s = max_wait_s
         self.tune = None if tune is None else nat.WfTune(*tune)
+        self.depth = 6 if self.tune is None else self.tune.steps_per_pass
+        self.region = (48, 128) if self.tune is None else (self.tune.tile_i, self.tune.tile_j)
         self.ctas_per_sm = ctas_per_sm
         self.stream = torch.cuda.current_stream(self.device)
         self.side = torch.cuda.Stream(self.device)
@@ -275,15 +310,20 @@ class Server:
     # ------------------------------------------------------------------
     def _admit(self) -> None:
         active = sum(L.nsol for L in self.live)
+        cells = sum(L.nsol * L.cells for L in self.live)
         while self.queue:
             tk = self.queue[0]
             fp = request_footprint(tk.request, self.chunk)
             nsol = len(tk.request.transmitters) * (2 if tk.request.target is not None else 1)
+            ncell = nsol * request_cells(tk.request)
             if self.used + fp > self.budget:
                 break   # arrival order: the head waits for memory
-            if self.live and active + nsol > self.max_active:
+            full = (active + nsol > self.max_active if self.mode == "persistent"
+                    else cells + ncell > self.max_cells)
+            if self.live and full:
                 break   # the GPU is full: the head waits for a slot
             active += nsol
+            cells += ncell
             self.queue.pop(0)
             L = _Live(self, tk)
             self.used += L.bytes
@@ -291,37 +331,80 @@ class Server:
             tk.status, tk.t_admit = "running", self.now()
             self.live.append(L)
 
+    def _host_buffer(self, nbytes: int) -> torch.Tensor:
+        """One of two pinned staging buffers, alternating per chunk (the chunk
+        that used a buffer two rounds ago has finished when step() returns)."""
+        self._hb_turn = 1 - getattr(self, "_hb_turn", 0)
+        bufs = self.__dict__.setdefault("_hb", [None, None])
+        b = bufs[self._hb_turn]
+        if b is None or b.numel() < nbytes:
+            b = torch.empty(max(nbytes, 1 << 20) * 2, dtype=torch.uint8, pin_memory=True)
+            bufs[self._hb_turn] = b
+        return b
+
     def _launch_chunk(self) -> None:
         if not self.live:
             return
-        descs, sizes = [], []
+        dsz = ctypes.sizeof(nat.WfSolve2D)
+        o_step0 = nat.WfSolve2D.step0.offset // 4
+        groups: dict = {}        # steps of this chunk -> [(request, first descriptor index)]
+        nsol = 0
         for L in self.live:
             ns = min(self.chunk, L.N - L.done)
             if L.grad:
                 L.ckpt[:, L.done // self.chunk].copy_(L.state[:L.ntx])
-            for d in L.desc:
-                d.step0 = L.done
-                d.nsteps = ns
-                d.status = 0
-                descs.append(d)
-                sizes.append(L.cells)
+            groups.setdefault(ns, []).append((L, nsol))
+            v = L.desc_np.view(np.int32).reshape(L.nsol, dsz // 4)
+            v[:, o_step0] = L.done
+            v[:, o_step0 + 1] = ns
+            v[:, o_step0 + 3] = 0
+            nsol += L.nsol
             self.cell_updates += L.nsol * L.cells * ns
             L.done += ns
-        n = len(descs)
-        arr = (nat.WfSolve2D * n)(*descs)
-        raw = torch.frombuffer(bytearray(bytes(memoryview(arr).cast("B"))), dtype=torch.uint8)
-        order = sorted(range(n), key=lambda q: -sizes[q])
-        host = torch.cat([raw, torch.tensor(order, dtype=torch.int32).view(torch.uint8)]).pin_memory()
-        dev = host.to(self.device, non_blocking=True)
-        self.h2d_bytes += host.numel()
+        chunks = [L.desc_np for L in self.live]
+        offs, plans = {}, {}
+        off = nsol * dsz
+        if self.mode == "persistent":
+            sizes = np.concatenate([np.full(L.nsol, L.cells) for L in self.live])
+            chunks.append(np.argsort(-sizes, kind="stable").astype(np.int32).view(np.uint8))
+        else:
+            for ns, members in groups.items():
+                plan = PassPlan(ns, self.depth)
+                plans[ns] = plan
+                for k in {plan.length(p) for p in range(plan.passes)}:
+                    rows = []
+                    for L, q0 in members:
+                        r = L.tile_rows(k, self.region).copy()
+                        r[:, 0] += q0
+                        rows.append(r)
+                    it = np.concatenate(rows)
+                    offs[(ns, k)] = (off, it.shape[0])
+                    b = it.view(np.uint8).reshape(-1)
+                    chunks.append(b)
+                    off += b.size
+        blob = np.concatenate(chunks)
+        host = self._host_buffer(blob.size)
+        host[:blob.size].numpy()[:] = blob
+        dev = host[:blob.size].to(self.device, non_blocking=True)
+        self.h2d_bytes += blob.size
         self._keep = dev
-        self._queue_ctr.zero_()
         fast = all(L.fast for L in self.live)
-        nat.check(nat.load().wf_batch2d_run(
-            dev.data_ptr(), n, dev.data_ptr() + raw.numel(), self._queue_ctr.data_ptr(),
-            None if self.tune is None else ctypes.byref(self.tune), self.ctas_per_sm,
-            1 if fast else 0, nat.stream_handle(self.device)))
-        self.launches += 1
+        stream = nat.stream_handle(self.device)
+        if self.mode == "persistent":
+            self._queue_ctr.zero_()
+            nat.check(nat.load().wf_batch2d_run(
+                dev.data_ptr(), nsol, dev.data_ptr() + nsol * dsz, self._queue_ctr.data_ptr(),
+                None if self.tune is None else ctypes.byref(self.tune), self.ctas_per_sm,
+                1 if fast else 0, stream))
+            self.launches += 1
+        else:
+            for ns, plan in plans.items():
+                items = {k: (dev.data_ptr() + o, c) for (g, k), (o, c) in offs.items() if g == ns}
+                run_tiled_passes(dev.data_ptr(), items, plan, self.tune, fast, stream)
+                self.launches += plan.passes
+                if plan.needs_copy:
+                    for L, _ in groups[ns]:
+                        L.state.copy_(L.scratch)
         ev = torch.cuda.Event(enable_timing=True)
         ev.record(self.stream)
         self._chunk_events.append((ev, self.now(), self.cell_updates))
@@ -350,39 +433,26 @@ class Server:
 
     def _adjoint(self, L: _Live) -> None:
         """Adjoint of a finished gradient request, enqueued on the side stream."""
+        from .adjoint import adjoint_runs
         lib = nat.load()
         st = self.side.cuda_stream
-        dev, K, N, cells = self.device, self.chunk, L.N, L.cells
+        dev, N, cells = self.device, L.N, L.cells
         model, target = L.traces[:L.ntx], L.traces[L.ntx:]
         resid = (model - target).contiguous()
         loss = 0.5 * ((model.double() - target.double()) ** 2).sum()
-        gca = torch.zeros(cells, dtype=torch.float64, device=dev)
+        gca = torch.zeros((L.ntx, cells), dtype=torch.float64, device=dev)
         gcb = torch.zeros_like(gca)
-        states = torch.empty((min(K, N) + 1, 3, cells), dtype=torch.float32, device=dev)
-        lam = torch.empty((3, cells), dtype=torch.float32, device=dev)
-        lam_s = torch.empty_like(lam)
         ca, cb = L.coef[0, 0], L.coef[0, 1]
+        keep: list = []
         ssz = ctypes.sizeof(nat.WfSource)
-        for t in range(L.ntx):
-            lam.zero_()
-            src = L.src_dev.data_ptr() + t * ssz
-            r = resid[t]
-            for s in reversed(range(L.nseg)):
-                s0 = s * K
-                ns = min(K, N - s0)
-                states[0].copy_(L.ckpt[t, s])
-                nat.check(lib.wf_fdtd2d_states(ctypes.byref(L.g), states.data_ptr(), ns,
-                                               ca.data_ptr(), cb.data_ptr(), src, 1, s0, st))
-                nat.check(lib.wf_adjoint2d_run(ctypes.byref(L.g), states.data_ptr(), ns,
-                                               ca.data_ptr(), cb.data_ptr(), L.probes.ptr,
-                                               L.probes.count, r.data_ptr(), r.stride(0), 0, s0,
-                                               lam.data_ptr(), lam_s.data_ptr(), gca.data_ptr(),
-                                               gcb.data_ptr(), st))
+        srcs = [_SrcView(L.src_dev, t * ssz) for t in range(L.ntx)]
+        adjoint_runs(L.g, cells, N, self.chunk, ca, cb, L.ckpt, resid, srcs, L.probes, gca, gcb,
+                     dev, stream=st, keep=keep)
         geps = torch.empty(cells, dtype=torch.float64, device=dev)
         gsig = torch.empty_like(geps)
         nat.check(lib.wf_material_grad(L.eps.data_ptr(), L.sig.data_ptr(), cells, L.grid.dt,
-                                       gca.data_ptr(), gcb.data_ptr(), 1.0, geps.data_ptr(),
-                                       gsig.data_ptr(), st))
+                                       gca.data_ptr(), gcb.data_ptr(), L.ntx, 1.0,
+                                       geps.data_ptr(), gsig.data_ptr(), st))
         L.host_traces = torch.empty((L.ntx, L.nrx, N), dtype=torch.float32, pin_memory=True)
         L.host_traces.copy_(model, non_blocking=True)
         L.host_grad = torch.empty((3, cells), dtype=torch.float64, pin_memory=True)
@@ -390,7 +460,7 @@ class Server:
         L.host_grad[1].copy_(gsig, non_blocking=True)
         L.host_grad[2, :1].copy_(loss.reshape(1), non_blocking=True)
         self.d2h_bytes += L.host_traces.numel() * 4 + (2 * cells + 1) * 8
-        L.adj_keep = (resid, gca, gcb, states, lam, lam_s, geps, gsig)
+        L.adj_keep = (resid, gca, gcb, geps, gsig, keep)
         L.event = torch.cuda.Event(enable_timing=True)
         L.event.record(self.side)
 
