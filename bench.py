@@ -294,6 +294,10 @@ def pass_launches(nsteps, k):
     return passes + (passes % 2)
 
 
+def _tune_arg(args):
+    return None if args.tune is None else tuple(int(v) for v in args.tune.split(","))
+
+
 def build_single(args, dev):
     """The solve of --workload plain2d / head3d: returns (sim, detectors,
     host (ca, cb), device (ca, cb), wave, cells, bytes per cell-update, oracle factory)."""
@@ -317,7 +321,8 @@ def build_single(args, dev):
         i, j = wl.source
         src = PointSource(_TableWave(wave), i, j, "Hz", grid=g, N_steps=wl.steps)
         cad, cbd = ca.to(dev), cb.to(dev)
-        sim = FDTD2D(g, f, MurABC(g, f.Hz), SourceCollection([src]), Ca=cad, Cb=cbd)
+        sim = FDTD2D(g, f, MurABC(g, f.Hz), SourceCollection([src]), Ca=cad, Cb=cbd,
+                     tune=_tune_arg(args))
         det = Detectors(wl.receivers)
 
         def make_oracle():
@@ -328,28 +333,36 @@ def build_single(args, dev):
         name = f"lossy_ellipses_{n}x{n}_{wl.steps}steps_16rx"
         return sim, det, (ca, cb), (cad, cbd), wave, n * n, 32, make_oracle, name, "k2d_pass"
 
-    wl = W.Head3D(n=args.side or 256, steps=args.nsteps)
+    B = max(1, args.instances)
+    wls = [W.Head3D(n=args.side or 256, steps=args.nsteps, seed=4 + q) for q in range(B)]
+    wl = wls[0]
     n = wl.n
     gh = YeeGrid(n, n, wl.dx, wl.dx, Nz=n, dz=wl.dx, courant=wl.courant, device="cpu")
-    mm = MaterialMap3D(gh, default=wl.background(Material))
-    wl.paint(mm, Material)
-    ca, cb = mm.build3d()
+    cas, cbs = [], []
+    for w in wls:
+        mm = MaterialMap3D(gh, default=w.background(Material))
+        w.paint(mm, Material)
+        a, c = mm.build3d()
+        cas.append(a)
+        cbs.append(c)
+    ca, cb = (cas[0], cbs[0]) if B == 1 else (torch.stack(cas), torch.stack(cbs))
     g = YeeGrid(n, n, wl.dx, wl.dx, Nz=n, dz=wl.dx, courant=wl.courant, device=dev)
-    f = FieldSet(g)
+    f = FieldSet(g, batch_size=B)
     wave = GaussianDerivativePulse(1e9).build(wl.steps, g.dt, dev)
     i, j, k = wl.source
     src = PointSource(_TableWave(wave), i, j, "Ez", k=k, grid=g, N_steps=wl.steps)
     cad, cbd = ca.to(dev), cb.to(dev)
-    sim = FDTD3D(g, f, MurABC3D(g, f.Hx, f.Hy, f.Hz), SourceCollection([src]), Ca=cad, Cb=cbd)
+    sim = FDTD3D(g, f, MurABC3D(g, f.Hx, f.Hy, f.Hz), SourceCollection([src]), Ca=cad, Cb=cbd,
+                 tune=_tune_arg(args))
     det = Detectors([("Ez",) + tuple(r) for r in wl.receivers()])
 
     def make_oracle():
-        o = oracle.Oracle3D(n, n, n, wl.dx, wl.dx, wl.dx, gh.dt, ca, cb)
+        o = oracle.Oracle3D(n, n, n, wl.dx, wl.dx, wl.dx, gh.dt, cas[0], cbs[0])
         o.add_point_source("Ez", i, j, oracle.gauss_deriv_wave(wl.steps, gh.dt), k=k)
         return o, [("Ez",) + tuple(r) for r in wl.receivers()]
 
-    name = f"head3d_{n}^3_{wl.steps}steps_{wl.n_rx}rx"
-    return sim, det, (ca, cb), (cad, cbd), wave, n ** 3, 56, make_oracle, name, "k3d_pass"
+    name = f"head3d_{n}^3_{wl.steps}steps_{wl.n_rx}rx" + (f"_x{B}_instances" if B > 1 else "")
+    return sim, det, (ca, cb), (cad, cbd), wave, B * n ** 3, 56, make_oracle, name, "k3d_stream"
 
 
 def cpu_single_sample(make_oracle, cells, max_steps, budget_s=12.0):
@@ -384,7 +397,7 @@ def bench_single(args, ws, rank, local):
         return sim.run(nsteps, record=det)
 
     for _ in range(args.warmup):
-        one_step()
+        tr_shape = tuple(one_step().shape)
     torch.cuda.synchronize(dev)
     barrier(ws)
     clk = ClockSampler(local)
@@ -406,7 +419,7 @@ def bench_single(args, ws, rank, local):
     # e2e: coefficients and waveform from pinned host memory, traces back to the host
     ca_h, cb_h = (c.pin_memory() for c in host_c)
     wave_h = wave.cpu().pin_memory()
-    tr_h = torch.empty((len(det), nsteps), dtype=torch.float32, pin_memory=True)
+    tr_h = torch.empty(tr_shape, dtype=torch.float32, pin_memory=True)
 
     def e2e_step():
         dev_c[0].copy_(ca_h, non_blocking=True)
@@ -440,7 +453,8 @@ def bench_single(args, ws, rank, local):
                     "temporal blocking re-uses tiles on chip, so frac may exceed 1"}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_single_sample(make_oracle, cells, nsteps, args.ref_budget)
+        per_solve = cells // sim.fields.batch_size
+        v, cores, sample = cpu_single_sample(make_oracle, per_solve, nsteps, args.ref_budget)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
     if rank == 0:
         line = {
@@ -549,7 +563,8 @@ def main():
                          "serve: Poisson request stream through the continuous-batching server")
     ap.add_argument("--batch-mode", default="persistent", choices=["persistent", "tiled"],
                     help="mimo: one persistent launch per batch, or one tile-queue launch per pass")
-    ap.add_argument("--tune", default=None, help="mimo: K,tile_i,tile_j,1,0 of the batched kernel")
+    ap.add_argument("--tune", default=None, help="K,tile_i,tile_j,tile_k,threads of the kernel (mimo: batched; plain2d/head3d: "
+                         "the solve's tune)")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: arrival window (s)")
     ap.add_argument("--max-wait", type=float, default=2.0, help="serve: wait bound (s)")
@@ -559,6 +574,8 @@ def main():
     ap.add_argument("--max-cells", type=float, default=3.2e7, help="serve: in-flight cell cap")
     ap.add_argument("--side", type=int, default=None,
                     help="grid side of plain2d (4096) / head3d (256)")
+    ap.add_argument("--instances", type=int, default=1,
+                    help="head3d: independent instances advanced in one launch per step")
     ap.add_argument("--phantoms", type=int, default=64)
     ap.add_argument("--tx", type=int, default=16)
     ap.add_argument("--nsteps", type=int, default=None,

@@ -179,6 +179,27 @@ int32_t wf_fdtd3d_run(const wf_grid3d* g,
                       int32_t n_check, uint32_t* check_max,
                       const wf_tune* tune, void* stream);
 
+/* Advance ninst independent 3D instances of one grid shape in ONE launch
+ * per step (the streaming kernel; tune NULL or tile_i == 0), e.g. a batched
+ * FieldSet (src/core/fields.py:97-101, 156-168: fields (B, Nx, Ny, Nz)) run
+ * by FDTD3D.step (src/core/fdtd3d.py:261-402, whose ellipsis updates act on
+ * every batch member).  Instance q uses f[c] + q*field_stride (and the same
+ * offset of s[c]), Ca/Cb + q*coef_stride (0 = shared), sources
+ * src[q*src_stride .. q*src_stride + src_per_inst) (src_stride 0 = every
+ * instance shares the list, as the reference's broadcast sources do,
+ * src/core/sources.py:885-887), traces + q*trace_stride; probes are the same
+ * points in every instance; check_max collects the maxima over all
+ * instances.  Other arguments as wf_fdtd3d_run. */
+int32_t wf_fdtd3d_batch_run(const wf_grid3d* g, int32_t ninst, int64_t field_stride,
+                            float* const* f, float* const* s,
+                            const float* ca, const float* cb, int64_t coef_stride,
+                            const wf_source* src, int32_t src_per_inst, int32_t src_stride,
+                            const wf_probe* probes, int32_t nprobe,
+                            float* traces, int64_t trace_ld, int64_t trace_stride,
+                            int32_t trace_step0, int32_t step0, int32_t nsteps,
+                            int32_t n_check, uint32_t* check_max,
+                            const wf_tune* tune, void* stream);
+
 /* One solve of a batched launch: an independent 2D TM grid with its own
  * state, scratch, coefficients, sources, probes and trace buffer.
  * Batching many of these is new functionality: the reference runs MIMO

@@ -17,7 +17,10 @@ from waveforge_b200 import (FDTD3D, Detectors, FieldSet, MurABC3D, PlaneSource, 
 pytestmark = pytest.mark.gpu
 
 COMPS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
-TUNES3 = [None, (1, 4, 4, 4, 64), (2, 3, 5, 7, 96), (3, 6, 6, 10, 128), (1, 8, 8, 30, 256)]
+# None = default (streaming kernel for Nz > 1); tile_i == 0 = streaming with
+# segments of tile_j planes; the rest select the tile kernel
+TUNES3 = [None, (1, 4, 4, 4, 64), (2, 3, 5, 7, 96), (3, 6, 6, 10, 128), (1, 8, 8, 30, 256),
+          (1, 0, 1, 0, 0), (1, 0, 3, 8, 0), (1, 0, 2, 16, 1), (1, 0, 0, 8, 1)]
 
 
 def sim3d(cuda, shape, dx, courant, srcs, ca=None, cb=None, steps=None, tune=None):
@@ -103,3 +106,77 @@ def test_random_3d_bit_exact_vs_oracle(cuda, seed):
         assert np.array_equal(tr.cpu().numpy(), tr_o.numpy()), tune
         for c in COMPS:
             assert np.array_equal(getattr(f, c).cpu().numpy(), getattr(o, c).numpy()), (tune, c)
+
+
+@pytest.mark.parametrize("mat", [False, True])
+def test_streaming_kernel_equals_tile_kernel_multi_block(cuda, mat):
+    """A volume spanning several 14 x 30 column blocks in j and k and several
+    i-segments: the streaming kernel (automatic and forced segment lengths)
+    equals the tile kernel bit for bit in traces, final fields and the
+    stability maxima, with E and H sources inside and across block edges."""
+    rng = np.random.default_rng(77 + mat)
+    shape = (23, 37, 71)
+    nx, ny, nz = shape
+    steps = 17
+    srcs = []
+    for c, (i, j, k) in (("Ez", (11, 14, 30)), ("Hy", (5, 15, 31)), ("Ex", (0, 0, 0)),
+                         ("Hx", (22, 36, 70)), ("Ey", (12, 28, 59))):
+        srcs.append((c, (i, i + 1, j, j + 1, k, k + 1),
+                     torch.from_numpy(rng.standard_normal(steps).astype(np.float32))))
+    ca = cb = None
+    if mat:
+        ca = torch.from_numpy(rng.uniform(0.3, 1.0, shape).astype(np.float32))
+        cb = torch.from_numpy(rng.uniform(0.001, 0.1, shape).astype(np.float32))
+    probes = [(COMPS[q % 6], int(rng.integers(0, nx)), int(rng.integers(0, ny)),
+               int(rng.integers(0, nz))) for q in range(24)]
+    probes += [("Hx", 0, 14, 30), ("Hz", 22, 0, 0), ("Ey", 11, 15, 29), ("Hy", 3, 36, 70)]
+    outs = []
+    for tune in ((1, 8, 8, 30, 256), None, (1, 0, 2, 0, 0), (1, 0, 7, 8, 0), (1, 0, 5, 16, 1),
+                 (1, 0, 0, 8, 1)):
+        sim, f = sim3d(cuda, shape, 1e-3, 0.9, srcs, ca, cb, steps=steps, tune=tune)
+        sim._n_check = 4
+        tr = sim.run(steps, record=Detectors(probes))
+        outs.append((tr.cpu(), [getattr(f, c).cpu() for c in COMPS], sim.last_field_max,
+                     sim.n_stability_checks))
+    ref = outs[0]
+    assert float(ref[0].abs().max()) > 0
+    for o in outs[1:]:
+        assert torch.equal(o[0], ref[0])
+        for a, b in zip(o[1], ref[1]):
+            assert torch.equal(a, b)
+        assert o[2] == ref[2] and o[3] == ref[3]
+
+
+def test_batched_instances_equal_separate_runs(cuda):
+    """A batched FieldSet (B, Nx, Ny, Nz) with per-member Ca/Cb runs in one
+    launch per step and equals B separate runs bit for bit (traces, fields,
+    stability maxima); sources reach every member, as the reference's
+    broadcast injection does."""
+    from waveforge_b200 import FieldSet as FS
+    rng = np.random.default_rng(909)
+    B, shape, steps = 3, (19, 33, 40), 12
+    nx, ny, nz = shape
+    ca = torch.from_numpy(rng.uniform(0.3, 1.0, (B,) + shape).astype(np.float32))
+    cb = torch.from_numpy(rng.uniform(0.001, 0.1, (B,) + shape).astype(np.float32))
+    wave = torch.from_numpy(rng.standard_normal(steps).astype(np.float32))
+    probes = [("Ez", 9, 16, 20), ("Hx", 0, 5, 39), ("Hy", 18, 32, 0), ("Ex", 4, 30, 31)]
+    g = YeeGrid(nx, ny, 1e-3, 1e-3, Nz=nz, dz=1e-3, courant=0.9, device=cuda)
+    f = FS(g, batch_size=B)
+    src = SourceCollection([PointSource(TabulatedWaveform(wave), 9, 16, "Ez", k=20, grid=g,
+                                        N_steps=steps)])
+    sim = FDTD3D(g, f, MurABC3D(g, f.Hx, f.Hy, f.Hz), src, Ca=ca.to(cuda), Cb=cb.to(cuda),
+                 n_check=5)
+    tr = sim.run(steps, record=Detectors(probes)).cpu()
+    assert tr.shape == (B, len(probes), steps)
+    maxima = []
+    for b in range(B):
+        s1, f1 = sim3d(cuda, shape, 1e-3, 0.9, [("Ez", (9, 10, 16, 17, 20, 21), wave)], ca[b],
+                       cb[b], steps=steps)
+        s1._n_check = 5
+        t1 = s1.run(steps, record=Detectors(probes)).cpu()
+        assert torch.equal(t1, tr[b])
+        for c in COMPS:
+            assert torch.equal(getattr(f1, c).cpu(), getattr(f, c)[b].cpu()), (b, c)
+        maxima.append(s1.last_field_max)
+    assert sim.last_field_max == max(maxima)
+    assert float(tr.abs().max()) > 0

@@ -22,7 +22,7 @@ WF_OK, WF_E_ARG, WF_E_CUDA, WF_E_LIMIT, WF_E_DIVERGED, WF_E_TIMEOUT = range(6)
 COMP_CODE = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
 
 EXPORTED = ("wf_abi_version", "wf_last_error", "wf_check_fastdiv", "wf_fdtd2d_run",
-            "wf_fdtd2d_run_noalloc", "wf_fdtd3d_run", "wf_batch2d_run", "wf_batch2d_pass", "wf_fdtd2d_states",
+            "wf_fdtd2d_run_noalloc", "wf_fdtd3d_run", "wf_fdtd3d_batch_run", "wf_batch2d_run", "wf_batch2d_pass", "wf_fdtd2d_states",
             "wf_adjoint2d_run", "wf_material_coeffs", "wf_material_grad", "wf_paint2d",
             "wf_das2d")
 NOALLOC_MAX_CELLS = 1 << 20   # WF_NOALLOC_MAX_CELLS of the header
@@ -112,6 +112,11 @@ def load() -> ctypes.CDLL:
         POINTER(WfGrid3D), POINTER(c_void_p), POINTER(c_void_p), c_void_p, c_void_p,
         c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int32, c_int32, c_int32,
         c_int32, c_void_p, POINTER(WfTune), c_void_p]
+    lib.wf_fdtd3d_batch_run.restype = c_int32
+    lib.wf_fdtd3d_batch_run.argtypes = [
+        POINTER(WfGrid3D), c_int32, c_int64, POINTER(c_void_p), POINTER(c_void_p), c_void_p,
+        c_void_p, c_int64, c_void_p, c_int32, c_int32, c_void_p, c_int32, c_void_p, c_int64,
+        c_int64, c_int32, c_int32, c_int32, c_int32, c_void_p, POINTER(WfTune), c_void_p]
     lib.wf_batch2d_run.restype = c_int32
     lib.wf_batch2d_run.argtypes = [c_void_p, c_int32, c_void_p, c_void_p, POINTER(WfTune),
                                    c_int32, c_int32, c_void_p]

@@ -103,9 +103,16 @@ class FDTD3D(EngineBase):
         chk, count = self._check_buffer(step0, nsteps)
         lib = nat.load()
         stream = nat.stream_handle(self._device)
+        f = self._fields
+        stream_tune = self._tune is None or self._tune.tile_i == 0
+        if f.is_batched and stream_tune and g.Nz > 1:
+            self._advance_batched(nsteps, src, probes, traces, chk, step0)
+            self.steps_completed += nsteps
+            self._process_checks(chk, count, step0)
+            return
         members = self._members()
         if probes is not None and len(members) > 1:
-            raise ValueError("Detectors.record supports unbatched FieldSets")
+            raise ValueError("Detectors.record on a batched FieldSet needs the default 3D tune")
         sp = (ctypes.c_void_p * 6)(*[self._scratch[c].data_ptr() for c in range(6)])
         for comps, ca, cb in members:
             for t in comps + ([ca, cb] if ca is not None else []):
@@ -122,6 +129,40 @@ class FDTD3D(EngineBase):
         self.steps_completed += nsteps
         self._process_checks(chk, count, step0)
 
+    def _advance_batched(self, nsteps, src, probes, traces, chk, step0) -> None:
+        """All batch members in one launch per step (wf_fdtd3d_batch_run):
+        every member gets the same sources, as the reference broadcasts them
+        (src/core/sources.py:885-887); Ca/Cb may be per member (B, Nx, Ny, Nz)
+        or shared (Nx, Ny, Nz)."""
+        g, f = self._grid, self._fields
+        n, B = g.Nx * g.Ny * g.Nz, f.batch_size
+        comps = [getattr(f, c) for c in FIELD_COMPONENTS]
+        for t in comps:
+            if not t.is_contiguous():
+                raise ValueError("batched field tensors must be contiguous (B, Nx, Ny, Nz)")
+        if self._scratch is None or self._scratch.numel() != 6 * B * n:
+            self._scratch = torch.empty((6, B, n), dtype=torch.float32, device=self._device)
+        ca, cb = self._Ca, self._Cb
+        cstride = 0
+        if ca is not None:
+            if not (ca.is_contiguous() and cb.is_contiguous()):
+                raise ValueError("Ca / Cb must be contiguous")
+            if ca.numel() == B * n:
+                cstride = n
+            elif ca.numel() != n:
+                raise ValueError("Ca / Cb must be (Nx, Ny, Nz) or (B, Nx, Ny, Nz)")
+        fp = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in comps])
+        sp = (ctypes.c_void_p * 6)(*[self._scratch[c].data_ptr() for c in range(6)])
+        nat.check(nat.load().wf_fdtd3d_batch_run(
+            ctypes.byref(self._g), B, n, fp, sp, nat.ptr(ca), nat.ptr(cb), cstride, src.ptr,
+            src.count, 0, None if probes is None else probes.ptr,
+            0 if probes is None else probes.count, None if traces is None else traces.data_ptr(),
+            0 if traces is None else traces.stride(-2),
+            0 if traces is None else traces.stride(0), step0, step0, nsteps,
+            self._n_check if chk is not None else 0, None if chk is None else chk.data_ptr(),
+            None if self._tune is None else ctypes.byref(self._tune),
+            nat.stream_handle(self._device)))
+
     def step(self) -> None:
         """Advance all six components one step in place (src/core/fdtd3d.py:261-402)."""
         self._advance(1)
@@ -136,12 +177,14 @@ class FDTD3D(EngineBase):
         probes = traces = None
         if record is not None:
             probes = record.table(self._device, FIELD_COMPONENTS, (g.Nx, g.Ny, g.Nz))
-            traces = torch.zeros((probes.count, n_steps), dtype=torch.float32, device=self._device)
+            shape = ((self._fields.batch_size,) if self._fields.is_batched else ()) + (probes.count,
+                                                                                     n_steps)
+            traces = torch.zeros(shape, dtype=torch.float32, device=self._device)
         chunk = max(1, n_steps // 10) if verbose else n_steps
         done = 0
         while done < n_steps:
             ns = min(chunk, n_steps - done)
-            self._advance(ns, probes, None if traces is None else traces[:, done:])
+            self._advance(ns, probes, None if traces is None else traces[..., done:])
             done += ns
             if verbose:
                 torch.cuda.synchronize(self._device)

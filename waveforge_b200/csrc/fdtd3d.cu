@@ -35,6 +35,10 @@ struct Tile3D {
   int n_check;
   unsigned* check_max;
   int check_base;
+  // batched instances (blockIdx.y; streaming kernel only): element strides
+  // between instances of the fields, coefficients (0 = shared) and traces
+  long long fstride, cstride, tstride;
+  int sstride;  // wf_source elements between instances' source lists (0 = shared)
 };
 
 struct Lists3D {
@@ -374,16 +378,397 @@ static int launch3(const Tile3D& P, const wf_tune& t, int s0, int k, cudaStream_
   return WF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// k3d_stream: one full time step as a 2.5D stream along i.
+//
+// A CTA owns a 16 (j) x 32 (k) block of columns -- a 14 x 30 core with a
+// one-cell halo on each side -- warp w = row j, lane = column k, one column
+// per thread, and walks a segment [ia, ib) of i-planes.  Each column keeps
+// its values in registers: old E of planes f..f+3 (prefetched two planes
+// ahead), old and curl-updated H of planes f-1..f+1.  In-plane neighbours come
+// from warp shuffles (k) and small shared exchange rows (j).
+// Iteration f: (A) Faraday update of plane p = f+1 (needs old E of p, p+1);
+// (B) Mur faces of plane f as pure functions of old and curl-updated H --
+// x faces read plane 1 (f = 0) or plane Nx-2 (f = Nx-1), then y faces read
+// row j=1 / Ny-2 through shared memory, then z faces read column k=1 / Nz-2
+// through shuffles (src/core/boundaries.py:499-583 order); (C) Ampere update
+// of plane f (needs final H of planes f and f-1) and the stores, detectors
+// and maxima of its core.  A segment starts one plane early (f0 = ia-1) to
+// have the final H of plane ia-1 without storing it.  Every float op is the
+// same separately rounded op, in the same order, as k3d_pass, so both
+// kernels are bit-identical to the reference.
+// ---------------------------------------------------------------------------
+constexpr int kSK = 32, kCK = kSK - 2;
+
+struct F3 {
+  float x, y, z;
+};
+
+template <int kSJ, bool DIRECT, bool MAT, bool FDIV>
+__global__ void __launch_bounds__(kSJ * kSK, 512 / (kSJ * kSK)) k3d_stream(Tile3D P, int tiles_j,
+                                                                          int tiles_k,
+                                                                          int seg_len, int n) {
+  constexpr int kCJ = kSJ - 2;
+  if (blockIdx.y) {
+    // this CTA's instance of a batched launch; sources: nsrc per instance
+    const long long q = blockIdx.y;
+    for (int c = 0; c < 6; ++c) {
+      P.in[c] += q * P.fstride;
+      P.out[c] += q * P.fstride;
+    }
+    if (P.ca) {
+      P.ca += q * P.cstride;
+      P.cb += q * P.cstride;
+    }
+    P.traces += q * P.tstride;
+    P.src += q * P.sstride;
+  }
+  __shared__ float sA[kSJ][kSK], sB[kSJ][kSK], sC[kSJ][kSK], sD[kSJ][kSK];
+  __shared__ Lists3D L;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int b = blockIdx.x;
+  const int tk = b % tiles_k;
+  b /= tiles_k;
+  const int tj = b % tiles_j, seg = b / tiles_j;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, tid = threadIdx.x;
+  const int gj = tj * kCJ - 1 + w, gk = tk * kCK - 1 + lane;
+  const bool in = gj >= 0 && gj < ny && gk >= 0 && gk < nz;
+  const bool core = in && w >= 1 && w <= kCJ && lane >= 1 && lane <= kCK;
+  const int ia = seg * seg_len, ib = min(nx, ia + seg_len);
+  if (ia >= ib) return;
+  const int f0 = max(ia - 1, 0);
+  const long long PS = (long long)ny * nz;
+  const long long col = in ? (long long)gj * nz + gk : 0;
+  const float dh = P.dh, de = P.de, dx = P.dx, dy = P.dy, dz = P.dz;
+  const float mx = P.mx, my = P.my, mz = P.mz;
+  const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy),
+               rdz = __drcp_rn((double)dz);
+  const int j0 = tj * kCJ - 1, k0 = tk * kCK - 1;
+  const bool yfaces = (j0 <= 0) || (j0 + kSJ >= ny);   // CTA-uniform
+
+  // ---- local source / probe lists -----------------------------------------
+  if (tid == 0) {
+    int nh = 0, ne = 0;
+    for (int q = 0; q < P.nsrc; ++q) {
+      const wf_source& S = P.src[q];
+      if (S.i1 <= f0 || S.i0 >= ib + 2 || S.j1 <= j0 || S.j0 >= j0 + kSJ || S.k1 <= k0 ||
+          S.k0 >= k0 + kSK)
+        continue;
+      if (S.comp >= WF_HX) {
+        if (nh < kMaxLocalSrc3) L.h[nh++] = (short)q;
+      } else {
+        if (ne < kMaxLocalSrc3) L.e[ne++] = (short)q;
+      }
+    }
+    L.nh = nh;
+    L.ne = ne;
+    L.np = 0;
+    for (int c = 0; c < 6; ++c) L.bmax[c] = 0u;
+  }
+  __syncthreads();
+  for (int q = tid; q < P.nprb; q += blockDim.x) {
+    const wf_probe& pr = P.prb[q];
+    if (pr.i >= ia && pr.i < ib && pr.j >= j0 + 1 && pr.j < j0 + 1 + kCJ && pr.k >= k0 + 1 &&
+        pr.k < k0 + 1 + kCK) {
+      const int slot = atomicAdd(&L.np, 1);
+      if (slot < kMaxLocalProbe3) L.p[slot] = (short)q;
+    }
+  }
+  __syncthreads();
+  const int ne = L.ne, nh = L.nh, np = min(L.np, kMaxLocalProbe3);
+
+  auto loadE = [&](int p) -> F3 {
+    F3 v{0.f, 0.f, 0.f};
+    if (in && p < nx) {
+      const long long o = (long long)p * PS + col;
+      v.x = P.in[0][o];
+      v.y = P.in[1][o];
+      v.z = P.in[2][o];
+      for (int q = 0; q < ne; ++q) {
+        const wf_source& S = P.src[L.e[q]];
+        if (p >= S.i0 && p < S.i1 && gj >= S.j0 && gj < S.j1 && gk >= S.k0 && gk < S.k1) {
+          const float s = src3_value(S, p, gj, gk, n);
+          if (S.comp == WF_EX) v.x = fadd(v.x, s);
+          else if (S.comp == WF_EY) v.y = fadd(v.y, s);
+          else v.z = fadd(v.z, s);
+        }
+      }
+    }
+    return v;
+  };
+  auto loadH = [&](int p) -> F3 {
+    F3 v{0.f, 0.f, 0.f};
+    if (in && p < nx) {
+      const long long o = (long long)p * PS + col;
+      v.x = P.in[3][o];
+      v.y = P.in[4][o];
+      v.z = P.in[5][o];
+    }
+    return v;
+  };
+  // Old Ex, Ez of plane p at row j+1 (the Faraday update's j neighbour),
+  // with the same source injection the neighbouring column applies.
+  const bool in_j1 = gj + 1 >= 0 && gj + 1 < ny && gk >= 0 && gk < nz;
+  auto loadJ1 = [&](int p) -> float2 {
+    float2 v{0.f, 0.f};
+    if (DIRECT && in_j1 && p < nx) {
+      const long long o = (long long)p * PS + (long long)(gj + 1) * nz + gk;
+      v.x = P.in[0][o];
+      v.y = P.in[2][o];
+      for (int q = 0; q < ne; ++q) {
+        const wf_source& S = P.src[L.e[q]];
+        if (p >= S.i0 && p < S.i1 && gj + 1 >= S.j0 && gj + 1 < S.j1 && gk >= S.k0 && gk < S.k1) {
+          const float s = src3_value(S, p, gj + 1, gk, n);
+          if (S.comp == WF_EX) v.x = fadd(v.x, s);
+          else if (S.comp == WF_EZ) v.y = fadd(v.y, s);
+        }
+      }
+    }
+    return v;
+  };
+  // Faraday update of plane p from its old E (e; j neighbour ej1 when
+  // DIRECT, else exchanged through sA/sB) and the old E of plane p+1 (en,
+  // own column).
+  auto curl = [&](int p, const F3& e, const F3& en, const F3& ho, const float2& ej1) -> F3 {
+    float ez_j, ex_j;
+    if (DIRECT) {
+      ex_j = ej1.x;
+      ez_j = ej1.y;
+    } else {
+      sA[w][lane] = e.x;
+      sB[w][lane] = e.z;
+      __syncthreads();
+      ez_j = w + 1 < kSJ ? sB[w + 1][lane] : 0.f;
+      ex_j = w + 1 < kSJ ? sA[w + 1][lane] : 0.f;
+    }
+    const float ey_k = __shfl_down_sync(0xffffffffu, e.y, 1);
+    const float ex_k = __shfl_down_sync(0xffffffffu, e.x, 1);
+    F3 v = ho;
+    for (int q = 0; q < nh; ++q) {
+      const wf_source& S = P.src[L.h[q]];
+      if (p >= S.i0 && p < S.i1 && gj >= S.j0 && gj < S.j1 && gk >= S.k0 && gk < S.k1) {
+        const float s = src3_value(S, p, gj, gk, n);
+        if (S.comp == WF_HX) v.x = fadd(v.x, s);
+        else if (S.comp == WF_HY) v.y = fadd(v.y, s);
+        else v.z = fadd(v.z, s);
+      }
+    }
+    if (gj < ny - 1 && gk < nz - 1) {
+      const float t1 = dv<FDIV>(fsub(ey_k, e.y), dz, rdz);
+      const float t2 = dv<FDIV>(fsub(ez_j, e.z), dy, rdy);
+      v.x = fadd(v.x, fmul(dh, fsub(t1, t2)));
+    }
+    if (p < nx - 1 && gk < nz - 1) {
+      const float t1 = dv<FDIV>(fsub(en.z, e.z), dx, rdx);
+      const float t2 = dv<FDIV>(fsub(ex_k, e.x), dz, rdz);
+      v.y = fadd(v.y, fmul(dh, fsub(t1, t2)));
+    }
+    if (p < nx - 1 && gj < ny - 1) {
+      const float t1 = dv<FDIV>(fsub(ex_j, e.x), dy, rdy);
+      const float t2 = dv<FDIV>(fsub(en.y, e.y), dx, rdx);
+      v.z = fadd(v.z, fmul(dh, fsub(t1, t2)));
+    }
+    return v;
+  };
+
+  // ---- prologue: planes f0, f0+1 ------------------------------------------
+  F3 e0 = loadE(f0), e1 = loadE(f0 + 1), e2 = loadE(f0 + 2), e3 = loadE(f0 + 3);
+  F3 h0o = loadH(f0), h1o = loadH(f0 + 1), h2o = loadH(f0 + 2);
+  float2 j0v = loadJ1(f0), j1v = loadJ1(f0 + 1), j2v = loadJ1(f0 + 2);
+  F3 h0c = curl(f0, e0, e1, h0o, j0v);
+  F3 h1c{0.f, 0.f, 0.f};
+  float hmo_y = 0.f, hmo_z = 0.f, hmc_y = 0.f, hmc_z = 0.f;  // plane f-1
+  F3 hprev{0.f, 0.f, 0.f};                                   // final H of plane f-1
+  float cav = 0.f, cbv = 0.f;
+  if (MAT && in) {
+    cav = P.ca[(long long)f0 * PS + col];
+    cbv = P.cb[(long long)f0 * PS + col];
+  }
+  unsigned mxb[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+  const bool check = P.check_max != nullptr && P.n_check > 0 && (n + 1) % P.n_check == 0;
+
+  for (int f = f0; f < ib; ++f) {
+    const int p = f + 1;
+    if (!DIRECT) __syncthreads();  // previous iteration's readers of sA/sB are done
+    // (A) Faraday update of plane p
+    if (p < nx) h1c = curl(p, e1, e2, h1o, j1v);
+    // (B) Mur faces of plane f
+    float hyx = h0c.y, hzx = h0c.z;
+    if (f == 0) {
+      hyx = fadd(h1o.y, fmul(mx, fsub(h1c.y, h0o.y)));
+      hzx = fadd(h1o.z, fmul(mx, fsub(h1c.z, h0o.z)));
+    } else if (f == nx - 1) {
+      hyx = fadd(hmo_y, fmul(mx, fsub(hmc_y, h0o.y)));
+      hzx = fadd(hmo_z, fmul(mx, fsub(hmc_z, h0o.z)));
+    }
+    float hxy = h0c.x, hzy = hzx;
+    if (yfaces) {
+      __syncthreads();  // readers of sA/sB in (A) are done
+      sA[w][lane] = h0c.x;
+      sB[w][lane] = hzx;
+      sC[w][lane] = h0o.x;
+      sD[w][lane] = h0o.z;
+      __syncthreads();
+      if (in && gj == 0 && w + 1 < kSJ) {
+        hxy = fadd(sC[w + 1][lane], fmul(my, fsub(sA[w + 1][lane], h0o.x)));
+        hzy = fadd(sD[w + 1][lane], fmul(my, fsub(sB[w + 1][lane], h0o.z)));
+      } else if (in && gj == ny - 1 && w >= 1) {
+        hxy = fadd(sC[w - 1][lane], fmul(my, fsub(sA[w - 1][lane], h0o.x)));
+        hzy = fadd(sD[w - 1][lane], fmul(my, fsub(sB[w - 1][lane], h0o.z)));
+      }
+    }
+    float hxF = hxy, hyF = hyx;
+    const float hx_dn = __shfl_down_sync(0xffffffffu, hxy, 1);
+    const float hxo_dn = __shfl_down_sync(0xffffffffu, h0o.x, 1);
+    const float hy_dn = __shfl_down_sync(0xffffffffu, hyx, 1);
+    const float hyo_dn = __shfl_down_sync(0xffffffffu, h0o.y, 1);
+    const float hx_up = __shfl_up_sync(0xffffffffu, hxy, 1);
+    const float hxo_up = __shfl_up_sync(0xffffffffu, h0o.x, 1);
+    const float hy_up = __shfl_up_sync(0xffffffffu, hyx, 1);
+    const float hyo_up = __shfl_up_sync(0xffffffffu, h0o.y, 1);
+    if (nz > 1 && in) {
+      if (gk == 0 && lane < 31) {
+        hxF = fadd(hxo_dn, fmul(mz, fsub(hx_dn, h0o.x)));
+        hyF = fadd(hyo_dn, fmul(mz, fsub(hy_dn, h0o.y)));
+      } else if (gk == nz - 1 && lane > 0) {
+        hxF = fadd(hxo_up, fmul(mz, fsub(hx_up, h0o.x)));
+        hyF = fadd(hyo_up, fmul(mz, fsub(hy_up, h0o.y)));
+      }
+    }
+    const float hzF = hzy;
+    // (C) Ampere update and outputs of plane f
+    if (f >= ia) {
+      __syncthreads();  // readers of sA/sB (A or B) are done
+      sA[w][lane] = hzF;
+      sB[w][lane] = hxF;
+      __syncthreads();
+      const float hy_k = __shfl_up_sync(0xffffffffu, hyF, 1);
+      const float hx_k = __shfl_up_sync(0xffffffffu, hxF, 1);
+      if (core) {
+        const float hz_j = sA[w - 1][lane], hx_j = sB[w - 1][lane];
+        float ex = e0.x, ey = e0.y, ez = e0.z;
+        if (gj >= 1 && gk >= 1) {
+          const float c = fsub(dv<FDIV>(fsub(hzF, hz_j), dy, rdy), dv<FDIV>(fsub(hyF, hy_k), dz, rdz));
+          ex = MAT ? fadd(fmul(cav, ex), fmul(cbv, c)) : fadd(ex, fmul(de, c));
+        }
+        if (f >= 1 && gk >= 1) {
+          const float c = fsub(dv<FDIV>(fsub(hxF, hx_k), dz, rdz), dv<FDIV>(fsub(hzF, hprev.z), dx, rdx));
+          ey = MAT ? fadd(fmul(cav, ey), fmul(cbv, c)) : fadd(ey, fmul(de, c));
+        }
+        if (f >= 1 && gj >= 1) {
+          const float c = fsub(dv<FDIV>(fsub(hyF, hprev.y), dx, rdx), dv<FDIV>(fsub(hxF, hx_j), dy, rdy));
+          ez = MAT ? fadd(fmul(cav, ez), fmul(cbv, c)) : fadd(ez, fmul(de, c));
+        }
+        const long long o = (long long)f * PS + col;
+        P.out[0][o] = ex;
+        P.out[1][o] = ey;
+        P.out[2][o] = ez;
+        P.out[3][o] = hxF;
+        P.out[4][o] = hyF;
+        P.out[5][o] = hzF;
+        for (int q = 0; q < np; ++q) {
+          const wf_probe& pr = P.prb[L.p[q]];
+          if (pr.i == f && pr.j == gj && pr.k == gk) {
+            const float v = pr.comp == WF_EX ? ex : pr.comp == WF_EY ? ey : pr.comp == WF_EZ ? ez
+                          : pr.comp == WF_HX ? hxF : pr.comp == WF_HY ? hyF : hzF;
+            P.traces[(long long)L.p[q] * P.trace_ld + (n - P.trace_step0)] = v;
+          }
+        }
+        if (check) {
+          mxb[0] = max(mxb[0], abs_bits(ex));
+          mxb[1] = max(mxb[1], abs_bits(ey));
+          mxb[2] = max(mxb[2], abs_bits(ez));
+          mxb[3] = max(mxb[3], abs_bits(hxF));
+          mxb[4] = max(mxb[4], abs_bits(hyF));
+          mxb[5] = max(mxb[5], abs_bits(hzF));
+        }
+      }
+    }
+    // (D) slide the plane window
+    hprev = F3{hxF, hyF, hzF};
+    hmo_y = h0o.y;
+    hmo_z = h0o.z;
+    hmc_y = h0c.y;
+    hmc_z = h0c.z;
+    h0o = h1o;
+    h0c = h1c;
+    h1o = h2o;
+    h2o = loadH(f + 3);
+    e0 = e1;
+    e1 = e2;
+    e2 = e3;
+    e3 = loadE(f + 4);
+    j1v = j2v;
+    j2v = loadJ1(f + 3);
+    if (MAT && in && f + 1 < nx) {
+      cav = P.ca[(long long)(f + 1) * PS + col];
+      cbv = P.cb[(long long)(f + 1) * PS + col];
+    }
+  }
+  if (check) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      for (int sh = 16; sh > 0; sh >>= 1) mxb[c] = max(mxb[c], __shfl_xor_sync(0xffffffffu, mxb[c], sh));
+      if (lane == 0) atomicMax(&L.bmax[c], mxb[c]);
+    }
+    __syncthreads();
+    if (tid < 6) {
+      const int idx = (n + 1) / P.n_check - P.check_base - 1;
+      atomicMax(&P.check_max[idx * 6 + tid], L.bmax[tid]);
+    }
+  }
+}
+
+template <int kSJ, bool DIRECT, bool MAT, bool FDIV>
+static int launch_stream_cfg(const Tile3D& P, int seg_len, int n, int nb, cudaStream_t st) {
+  constexpr int kCJ = kSJ - 2;
+  const int tiles_j = (P.ny + kCJ - 1) / kCJ, tiles_k = (P.nz + kCK - 1) / kCK;
+  const int nseg = (P.nx + seg_len - 1) / seg_len;
+  const long long nblk = (long long)tiles_j * tiles_k * nseg;
+  if (nblk > 0x7fffffffLL) return set_error(WF_E_LIMIT, "wf_fdtd3d_run: too many column blocks");
+  if (nb < 1 || nb > 65535) return set_error(WF_E_LIMIT, "wf_fdtd3d: 1..65535 instances");
+  dim3 grid((unsigned)nblk, (unsigned)nb);
+  k3d_stream<kSJ, DIRECT, MAT, FDIV><<<grid, kSJ * kSK, 0, st>>>(P, tiles_j, tiles_k, seg_len, n);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "launch k3d_stream");
+  return WF_OK;
+}
+
+// Streaming variants: rows per column block (16 = 512 threads, one CTA per
+// SM; 8 = 256 threads, two per SM) and whether the Faraday update reads its
+// j neighbour directly (no shared exchange, one CTA barrier less per plane).
+template <bool MAT, bool FDIV>
+static int launch_stream(const Tile3D& P, int seg_len, int n, int rows, bool direct, int nb,
+                         cudaStream_t st) {
+  if (rows == 8)
+    return direct ? launch_stream_cfg<8, true, MAT, FDIV>(P, seg_len, n, nb, st)
+                  : launch_stream_cfg<8, false, MAT, FDIV>(P, seg_len, n, nb, st);
+  return direct ? launch_stream_cfg<16, true, MAT, FDIV>(P, seg_len, n, nb, st)
+                : launch_stream_cfg<16, false, MAT, FDIV>(P, seg_len, n, nb, st);
+}
+
+// Segment length along i: enough column blocks for ~4 per SM, at least 8
+// planes per segment.
+static int stream_seg_len(int nx, int ny, int nz, int rows) {
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long plane = (long long)((ny + rows - 3) / (rows - 2)) * ((nz + kCK - 1) / kCK);
+  long long nseg = (4LL * nsm + plane - 1) / plane;
+  nseg = std::max(1LL, std::min(nseg, (long long)std::max(1, nx / 8)));
+  return (int)((nx + nseg - 1) / nseg);
+}
+
 }  // namespace wf
 
 using namespace wf;
 
-extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* const* s,
-                                 const float* ca, const float* cb, const wf_source* src,
-                                 int32_t nsrc, const wf_probe* probes, int32_t nprobe,
-                                 float* traces, int64_t trace_ld, int32_t trace_step0,
-                                 int32_t step0, int32_t nsteps, int32_t n_check,
-                                 uint32_t* check_max, const wf_tune* tune, void* stream) {
+static int run3d(const wf_grid3d* g, int nb, long long fstride, long long cstride,
+                 long long tstride, int sstride, float* const* f, float* const* s, const float* ca,
+                 const float* cb, const wf_source* src, int32_t nsrc, const wf_probe* probes,
+                 int32_t nprobe, float* traces, int64_t trace_ld, int32_t trace_step0,
+                 int32_t step0, int32_t nsteps, int32_t n_check, uint32_t* check_max,
+                 const wf_tune* tune, void* stream) {
   if (g == nullptr || f == nullptr || s == nullptr)
     return set_error(WF_E_ARG, "wf_fdtd3d_run: null grid/state/scratch array");
   for (int c = 0; c < 6; ++c)
@@ -400,9 +785,26 @@ extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* con
   if (nsrc > 32767 || nprobe > 32767)
     return set_error(WF_E_LIMIT, "wf_fdtd3d_run: at most 32767 sources and probes");
   if (nsteps == 0) return WF_OK;
+  // Default: the single-step streaming kernel (k3d_stream) for volumes, the
+  // tile kernel (k3d_pass) for Nz == 1.  An explicit tune with tile_i == 0
+  // selects streaming with segments of tile_j planes (0 = automatic); any
+  // other tune selects the tile kernel with that shape and depth.
   wf_tune t{};
-  if (tune) {
+  bool stream_k = false, direct = true;
+  int seg_len = 0, rows = 16;
+  if (tune && tune->tile_i == 0) {
+    // streaming: tile_j = segment length (0 = automatic), tile_k = rows per
+    // column block (8 or 16; 0 = 16), threads = 1 for the shared-memory
+    // j exchange instead of direct neighbour loads
+    stream_k = true;
+    seg_len = tune->tile_j;
+    rows = tune->tile_k == 8 ? 8 : 16;
+    direct = tune->threads != 1;
+    if (seg_len < 0) return set_error(WF_E_ARG, "wf_fdtd3d_run: negative segment length");
+  } else if (tune) {
     t = *tune;
+  } else if (g->nz > 1) {
+    stream_k = true;
   } else {
     t.steps_per_pass = 1;
     t.tile_i = 4;
@@ -410,9 +812,15 @@ extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* con
     t.tile_k = 30;
     t.threads = 256;
   }
-  if (t.steps_per_pass < 1 || t.steps_per_pass > 8 || t.tile_i < 2 || t.tile_j < 2 ||
-      t.tile_k < 2 || t.threads < 32 || t.threads > 512 || (t.threads & 31))
+  if (nb > 1 && !stream_k)
+    return set_error(WF_E_ARG, "wf_fdtd3d_batch_run: batched instances need the streaming kernel");
+  if (stream_k) {
+    t.steps_per_pass = 1;
+    if (seg_len == 0) seg_len = stream_seg_len(g->nx, g->ny, g->nz, rows);
+  } else if (t.steps_per_pass < 1 || t.steps_per_pass > 8 || t.tile_i < 2 || t.tile_j < 2 ||
+             t.tile_k < 2 || t.threads < 32 || t.threads > 512 || (t.threads & 31)) {
     return set_error(WF_E_ARG, "wf_fdtd3d_run: bad tune");
+  }
   cudaStream_t st = (cudaStream_t)stream;
   Tile3D P{};
   P.nx = g->nx;
@@ -438,6 +846,10 @@ extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* con
   P.n_check = n_check;
   P.check_max = check_max;
   P.check_base = n_check > 0 ? step0 / n_check : 0;
+  P.fstride = fstride;
+  P.cstride = cstride;
+  P.tstride = tstride;
+  P.sstride = sstride;
   const int all3 = WF_FASTDIV_X | WF_FASTDIV_Y | WF_FASTDIV_Z;
   const int all2 = WF_FASTDIV_X | WF_FASTDIV_Y;
   const bool fd = g->nz > 1 ? (g->flags & all3) == all3 : (g->flags & all2) == all2;
@@ -450,8 +862,15 @@ extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* con
       P.out[c] = out[c];
     }
     const int s0 = step0 + plan.offset(p), k = plan.len(p);
-    const int rc = ca ? (fd ? launch3<true, true>(P, t, s0, k, st) : launch3<true, false>(P, t, s0, k, st))
-                      : (fd ? launch3<false, true>(P, t, s0, k, st) : launch3<false, false>(P, t, s0, k, st));
+    int rc;
+    if (stream_k)
+      rc = ca ? (fd ? launch_stream<true, true>(P, seg_len, s0, rows, direct, nb, st)
+                    : launch_stream<true, false>(P, seg_len, s0, rows, direct, nb, st))
+              : (fd ? launch_stream<false, true>(P, seg_len, s0, rows, direct, nb, st)
+                    : launch_stream<false, false>(P, seg_len, s0, rows, direct, nb, st));
+    else
+      rc = ca ? (fd ? launch3<true, true>(P, t, s0, k, st) : launch3<true, false>(P, t, s0, k, st))
+              : (fd ? launch3<false, true>(P, t, s0, k, st) : launch3<false, false>(P, t, s0, k, st));
     if (rc) return rc;
   }
   if (plan.needs_copy()) {
@@ -459,9 +878,47 @@ extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* con
       P.in[c] = s[c];
       P.out[c] = f[c];
     }
-    k_copy6<<<592, 256, 0, st>>>(P, (long long)g->nx * g->ny * g->nz);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "launch k_copy6");
+    for (int q = 0; q < nb; ++q) {
+      k_copy6<<<592, 256, 0, st>>>(P, (long long)g->nx * g->ny * g->nz);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "launch k_copy6");
+      for (int c = 0; c < 6; ++c) {
+        P.in[c] += fstride;
+        P.out[c] += fstride;
+      }
+    }
   }
   return WF_OK;
+}
+
+extern "C" int32_t wf_fdtd3d_run(const wf_grid3d* g, float* const* f, float* const* s,
+                                 const float* ca, const float* cb, const wf_source* src,
+                                 int32_t nsrc, const wf_probe* probes, int32_t nprobe,
+                                 float* traces, int64_t trace_ld, int32_t trace_step0,
+                                 int32_t step0, int32_t nsteps, int32_t n_check,
+                                 uint32_t* check_max, const wf_tune* tune, void* stream) {
+  return run3d(g, 1, 0, 0, 0, 0, f, s, ca, cb, src, nsrc, probes, nprobe, traces, trace_ld,
+               trace_step0, step0, nsteps, n_check, check_max, tune, stream);
+}
+
+extern "C" int32_t wf_fdtd3d_batch_run(const wf_grid3d* g, int32_t ninst, int64_t field_stride,
+                                       float* const* f, float* const* s, const float* ca,
+                                       const float* cb, int64_t coef_stride,
+                                       const wf_source* src, int32_t src_per_inst,
+                                       int32_t src_stride,
+                                       const wf_probe* probes, int32_t nprobe, float* traces,
+                                       int64_t trace_ld, int64_t trace_stride,
+                                       int32_t trace_step0, int32_t step0, int32_t nsteps,
+                                       int32_t n_check, uint32_t* check_max,
+                                       const wf_tune* tune, void* stream) {
+  if (g == nullptr || ninst < 1 || ninst > 65535)
+    return set_error(WF_E_ARG, "wf_fdtd3d_batch_run: null grid or instance count outside 1..65535");
+  const long long n = (long long)g->nx * g->ny * g->nz;
+  if (ninst > 1 && (field_stride < n || (ca != nullptr && coef_stride != 0 && coef_stride < n) ||
+                    (nprobe > 0 && trace_stride < (long long)nprobe * trace_ld) ||
+                    src_stride < 0 || (src_stride > 0 && src_stride < src_per_inst)))
+    return set_error(WF_E_ARG, "wf_fdtd3d_batch_run: instance strides overlap");
+  return run3d(g, ninst, field_stride, coef_stride, trace_stride, src_stride, f, s, ca, cb, src,
+               src_per_inst, probes, nprobe, traces, trace_ld, trace_step0, step0, nsteps,
+               n_check, check_max, tune, stream);
 }
