@@ -551,16 +551,94 @@ def bench_serve(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# adjoint: one misfit gradient (forward with checkpoints + reverse pass)
+# ---------------------------------------------------------------------------
+
+def bench_adjoint(args, ws, rank, local):
+    from waveforge_b200 import MisfitProblem2D, PointSource, SourceCollection, YeeGrid, fdtd_misfit
+    from waveforge_b200 import workloads as W
+    from waveforge_b200.core.sources import TabulatedWaveform
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    side, steps = args.side or 512, args.nsteps
+    req = W.serving_request(side, steps, args.seed, gradient=True)
+    gh = req.material._grid
+    g = YeeGrid(side, side, gh.dx, gh.dy, courant=gh.courant, device=dev)
+    wave = TabulatedWaveform(req.waveform.build(steps, g.dt, "cpu"))
+    srcs = [SourceCollection([PointSource(wave, i, j, "Hz", grid=g, N_steps=steps)])
+            for i, j in req.transmitters]
+    n_tx, n_rx = len(srcs), len(req.receivers)
+    eps_t = torch.empty((side, side), dtype=torch.float64, device=dev)
+    sig_t = torch.empty_like(eps_t)
+    req.target.build_device(dev, eps_sigma=(eps_t, sig_t))
+    tp = MisfitProblem2D(g, srcs, list(req.receivers), torch.zeros(n_tx, n_rx, steps), steps)
+    with torch.no_grad():
+        fdtd_misfit(eps_t, sig_t, tp)
+    prob = MisfitProblem2D(g, srcs, list(req.receivers), tp.traces, steps)
+    eps = torch.empty_like(eps_t)
+    sig = torch.empty_like(eps_t)
+    req.material.build_device(dev, eps_sigma=(eps, sig))
+
+    def one():
+        e = eps.clone().requires_grad_(True)
+        s = sig.clone().requires_grad_(True)
+        a = torch.cuda.Event(enable_timing=True)
+        m = torch.cuda.Event(enable_timing=True)
+        z = torch.cuda.Event(enable_timing=True)
+        a.record()
+        loss = fdtd_misfit(e, s, prob)
+        m.record()
+        loss.backward()
+        z.record()
+        return a, m, z, e.grad
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clk = ClockSampler(local)
+    clk.start()
+    fw, bw, tot = [], [], []
+    for _ in range(args.steps):
+        a, m, z, gr = one()
+        torch.cuda.synchronize(dev)
+        fw.append(a.elapsed_time(m))
+        bw.append(m.elapsed_time(z))
+        tot.append(a.elapsed_time(z))
+    clocks = clk.stop()
+    ms = reduce_max(statistics.mean(tot), ws, dev)
+    upd = n_tx * side * side * steps
+    if rank == 0:
+        line = {
+            "metric": "gradient Gcell-upd/s (misfit forward + adjoint, fp32)",
+            "value": ws * upd / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"adjoint_lossy_{side}x{side}_{steps}steps_{n_tx}tx",
+                       "checkpoint_every": prob.K, "parallelism": f"replicas x{ws}",
+                       "note": "value counts the forward cell-updates of the model phantom; "
+                               "one step = forward with sqrt(N) checkpoints + reverse pass "
+                               "(segment recompute + time-reversed Yee step per step)"},
+            "forward_ms": statistics.mean(fw), "backward_ms": statistics.mean(bw),
+            "backward_over_forward": statistics.mean(bw) / statistics.mean(fw),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mimo", choices=["mimo", "plain2d", "head3d", "serve"],
+    ap.add_argument("--workload", default="mimo", choices=["mimo", "plain2d", "head3d", "serve", "adjoint"],
                     help="mimo: batched uneven breast MIMO (default, the headline metric); "
                          "plain2d: one 4096^2 lossy 2D solve; head3d: one 256^3 head solve; "
-                         "serve: Poisson request stream through the continuous-batching server")
+                         "serve: Poisson request stream through the continuous-batching server; "
+                         "adjoint: one misfit gradient (forward + adjoint) of a 512^2 16-TX phantom")
     ap.add_argument("--batch-mode", default="persistent", choices=["persistent", "tiled"],
                     help="mimo: one persistent launch per batch, or one tile-queue launch per pass")
     ap.add_argument("--tune", default=None, help="K,tile_i,tile_j,tile_k,threads of the kernel (mimo: batched; plain2d/head3d: "
@@ -588,10 +666,15 @@ def main():
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
     if args.nsteps is None:
-        args.nsteps = {"mimo": 3000, "plain2d": 2000, "head3d": 1500, "serve": 0}[args.workload]
+        args.nsteps = {"mimo": 3000, "plain2d": 2000, "head3d": 1500, "serve": 0,
+                       "adjoint": 1000}[args.workload]
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
+        barrier(ws)
+        return
+    if args.workload == "adjoint":
+        bench_adjoint(args, ws, rank, local)
         barrier(ws)
         return
     if args.workload == "serve":

@@ -31,7 +31,7 @@ from typing import Optional, Sequence
 import torch
 
 from . import _native as nat
-from .batch import grid_struct
+from .batch import PassPlan, grid_struct, run_tiled_passes, tile_items
 from .core._engine import ProbeTable, SourceTable, source_list
 from .core.grid import YeeGrid
 from .detectors import Detectors
@@ -107,30 +107,53 @@ class MisfitProblem2D:
 
     def forward_runs(self, ca: torch.Tensor, cb: torch.Tensor, keep_checkpoints: bool):
         """Run every transmitter; returns (traces (n_tx, n_rx, N), checkpoints
-        (n_tx, n_seg, 3, Nx, Ny) or None)."""
+        (n_tx, n_seg, 3, Nx, Ny) or None).  All transmitters advance together:
+        each temporal pass of a segment is one wf_batch2d_pass over the tiles
+        of every transmitter's grid (same tile routine as wf_fdtd2d_run, so
+        the traces are those of the plain per-transmitter runs)."""
         g, dev, N, K = self.grid, self.device, self.n_steps, self.K
-        lib = nat.load()
-        stream = nat.stream_handle(dev)
         n_tx, n_rx = len(self.sources), len(self.detectors)
+        cells = g.Nx * g.Ny
         traces = torch.zeros((n_tx, n_rx, N), dtype=torch.float32, device=dev)
-        fields = torch.empty((3, g.Nx, g.Ny), dtype=torch.float32, device=dev)
-        scratch = torch.empty_like(fields)
+        state = torch.zeros((n_tx, 3, cells), dtype=torch.float32, device=dev)
+        scratch = torch.empty_like(state)
         ckpt = (torch.empty((n_tx, self.n_segments, 3, g.Nx, g.Ny), dtype=torch.float32,
                             device=dev) if keep_checkpoints else None)
+        desc = (nat.WfSolve2D * n_tx)()
         for t, st in enumerate(self.sources):
-            fields.zero_()
-            tr = traces[t]
-            seg_len = K if keep_checkpoints else N
-            for s0 in range(0, N, seg_len):
-                if keep_checkpoints:
-                    ckpt[t, s0 // K].copy_(fields)
-                ns = min(seg_len, N - s0)
-                nat.check(lib.wf_fdtd2d_run(
-                    ctypes.byref(self.g), fields[0].data_ptr(), fields[1].data_ptr(),
-                    fields[2].data_ptr(), scratch[0].data_ptr(), scratch[1].data_ptr(),
-                    scratch[2].data_ptr(), ca.data_ptr(), cb.data_ptr(), st.ptr, st.count,
-                    self.probes.ptr, self.probes.count, tr.data_ptr(), tr.stride(0), 0, s0, ns, 0,
-                    None, None, stream))
+            d = desc[t]
+            d.g = self.g
+            d.ex, d.ey, d.hz = (state[t, c].data_ptr() for c in range(3))
+            d.sx, d.sy, d.sz = (scratch[t, c].data_ptr() for c in range(3))
+            d.ca, d.cb = ca.data_ptr(), cb.data_ptr()
+            d.src, d.nsrc = st.ptr, st.count
+            d.probes, d.nprobe = self.probes.ptr, self.probes.count
+            d.traces, d.trace_ld, d.trace_step0 = traces[t].data_ptr(), N, 0
+            d.n_check, d.check_max = 0, None
+        both = nat.WF_FASTDIV_X | nat.WF_FASTDIV_Y
+        fast = (self.g.flags & both) == both
+        stream = nat.stream_handle(dev)
+        seg_len = K if keep_checkpoints else N
+        items: dict = {}
+        keep = []
+        for s0 in range(0, N, seg_len):
+            if keep_checkpoints:
+                ckpt[:, s0 // K].copy_(state.view(n_tx, 3, g.Nx, g.Ny))
+            ns = min(seg_len, N - s0)
+            for d in desc:
+                d.step0, d.nsteps, d.status = s0, ns, 0
+            dd = nat.to_device_bytes(desc, dev)
+            keep.append(dd)
+            plan = PassPlan(ns, 6)
+            for q in range(plan.passes):
+                k = plan.length(q)
+                if k not in items:
+                    it = torch.from_numpy(tile_items([(g.Nx, g.Ny)] * n_tx, k, (48, 128))).to(dev)
+                    items[k] = (it, it.shape[0])
+            run_tiled_passes(dd.data_ptr(), {k: (t.data_ptr(), c) for k, (t, c) in items.items()},
+                             plan, None, fast, stream)
+            if plan.needs_copy:
+                state.copy_(scratch)
         return traces, ckpt
 
     def adjoint(self, ca, cb, ckpt, resid):
