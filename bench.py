@@ -3,8 +3,9 @@
 Workload (one bench "step"): 64 seeded breast phantoms (sides drawn from
 {150,200,256,384,512}, dx = 0.5 mm, Courant 0.5), each with a 16-antenna
 ring; every transmitter is a separate 3000-step solve recording 16 receivers,
-for the tumour phantom AND its healthy twin (2 x 1024 solves, each batch one
-persistent launch), followed by one 128x128 DAS image per phantom of
+for the tumour phantom AND its healthy twin (2 x 1024 solves; each batch's
+launch shape is picked by the autotuner and its whole run replayed from a
+CUDA graph), followed by one 128x128 DAS image per phantom of
 S_tumour - S_healthy.  Metric: aggregate Gcell-updates/s (cells x steps of all
 solves / time).  Inputs (fields 2 x 1.3 GB) are far larger than L2, so no L2
 flush is needed between steps.
@@ -639,8 +640,11 @@ def main():
                          "plain2d: one 4096^2 lossy 2D solve; head3d: one 256^3 head solve; "
                          "serve: Poisson request stream through the continuous-batching server; "
                          "adjoint: one misfit gradient (forward + adjoint) of a 512^2 16-TX phantom")
-    ap.add_argument("--batch-mode", default="persistent", choices=["persistent", "tiled"],
-                    help="mimo: one persistent launch per batch, or one tile-queue launch per pass")
+    ap.add_argument("--batch-mode", default="auto", choices=["persistent", "tiled", "auto"],
+                    help="mimo: one persistent launch per batch, one tile-queue launch per pass, "
+                         "or the autotuner's pick (default)")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="mimo: launch each run directly instead of replaying its CUDA graph")
     ap.add_argument("--tune", default=None, help="K,tile_i,tile_j,tile_k,threads of the kernel (mimo: batched; plain2d/head3d: "
                          "the solve's tune)")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
@@ -702,19 +706,29 @@ def main():
 
     kern_ms = []
 
-    def one_step(record=False):
+    if args.graph:
         for b in batches.values():
-            b.reset()
+            b.capture()
+
+    def one_step(record=False):
+        if not args.graph:
+            for b in batches.values():
+                b.reset()
         ev = []
         for t in (True, False):
             b = batches[t]
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
-            b._upload(0, args.nsteps)
-            e0.record(stream)
-            b.launch()
-            e1.record(stream)
-            b.step = args.nsteps
+            if args.graph:
+                e0.record(stream)
+                b.replay()
+                e1.record(stream)
+            else:
+                b._upload(0, args.nsteps)
+                e0.record(stream)
+                b.launch()
+                e1.record(stream)
+                b.step = args.nsteps
             ev.append((e0, e1))
         das_all(batches, phantoms, wl, args.tx, dev, images)
         return ev
@@ -826,13 +840,13 @@ def main():
     k_ms = statistics.mean(kern_ms)
     achieved = BYTES_PER_CELL_UPDATE * (cells_per_step / 2) / (k_ms * 1e-3) / 1e9
     traffic = None
-    tfile = ROOT / "profiles" / ("k_batch2d_traffic.txt" if args.batch_mode == "persistent"
+    tfile = ROOT / "profiles" / ("k_batch2d_traffic.txt" if batches[True].mode == "persistent"
                                  else "k_batch_pass_traffic.txt")
     if tfile.exists():
         for line in tfile.read_text().splitlines():
             if line.startswith("dram_bytes_per_cell_update="):
                 traffic = float(line.split("=")[1]) * cells_per_step / 2
-    kname = "k_batch2d" if args.batch_mode == "persistent" else "k_batch_pass"
+    kname = "k_batch2d" if batches[True].mode == "persistent" else "k_batch_pass"
     roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
             "bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
@@ -855,7 +869,9 @@ def main():
                        "twins": "tumour + healthy", "das": f"{len(phantoms)} x {DAS_SIZE}x{DAS_SIZE}",
                        "cell_updates_per_step": cells_per_step, "grid_sides": "150-512",
                        "dx_mm": 0.5, "courant": 0.5, "l2": "inputs > L2 (2.6 GB fields), no flush",
-                       "batch_mode": args.batch_mode, "tune": args.tune,
+                       "batch_mode": batches[True].mode, "graph": args.graph,
+                       "tune": args.tune if args.batch_mode != "auto" else
+                       [batches[True].depth, *batches[True].region],
                        "parallelism": f"replicas x{ws}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},

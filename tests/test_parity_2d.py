@@ -284,3 +284,46 @@ def test_full_size_linearity_and_tune_independence(cuda):
     assert torch.allclose(outs[1][1], 2.0 * outs[0][1], rtol=0.0, atol=1e-36)
     assert torch.equal(outs[2][0], outs[0][0])
     assert torch.equal(outs[2][1], outs[0][1])
+
+
+def test_batch_graph_replay_and_autotune_bit_exact(cuda):
+    """A CUDA-graph capture of a full batched run replays to the same bits as
+    the plain runs (both scheduling modes, two replays in a row), and the
+    autotuned batch (whatever shape it picks) gives the same bits too."""
+    g = load("breast_mimo_small")
+    steps = 120
+    wave = torch.from_numpy(g["wave"][:steps].copy())
+    solves, refs = [], []
+    for p in range(len(g["sides"])):
+        ph, ca, cb = breast_coeffs(g, p)
+        ant = ph.antennas(16)
+        for tx in range(3):
+            i, j = ant[tx]
+            grid = YeeGrid(ph.side, ph.side, float(g["dx"]), float(g["dx"]),
+                           courant=float(g["courant"]), device=cuda)
+            src = PointSource(TabulatedWaveform(wave), i, j, "Hz", grid=grid, N_steps=steps)
+            solves.append(BatchSolve(grid, SourceCollection([src]), Detectors(ant),
+                                     ca.reshape(ph.side, ph.side, 1).to(cuda),
+                                     cb.reshape(ph.side, ph.side, 1).to(cuda)))
+            sim, f = sim2d(cuda, ph.side, ph.side, float(g["dx"]), float(g["courant"]),
+                           [("Hz", "point", (i, i + 1, j, j + 1), wave, None)], ca, cb,
+                           steps=steps)
+            refs.append((sim.run(steps, record=Detectors(ant)).clone(), f.Hz.clone()))
+    for mode in ("persistent", "tiled"):
+        b = Batch2D(solves, steps, mode=mode)
+        b.capture()
+        for _ in range(2):
+            b.replay()
+            torch.cuda.synchronize()
+            for q, (tr, hz) in enumerate(refs):
+                assert torch.equal(b.traces(q), tr), (mode, q)
+                assert torch.equal(b.fields(q)[2].reshape(hz.shape), hz), (mode, q)
+    auto = Batch2D(solves, steps, tune="auto")
+    assert auto.mode in ("persistent", "tiled")
+    auto.run()
+    torch.cuda.synchronize()
+    for q, (tr, hz) in enumerate(refs):
+        assert torch.equal(auto.traces(q), tr)
+    from waveforge_b200.autotune import tune_plain2d
+    t = tune_plain2d(300, 200, materials=True, device=cuda)
+    assert len(t) == 5 and t[0] >= 1

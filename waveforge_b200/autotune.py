@@ -1,0 +1,141 @@
+"""Launch-shape autotuner for the batched and plain 2D paths.
+
+The reference has nothing to tune (it runs PyTorch eager ops).  Here the
+temporal-block depth K, the register layout of the tile (region RH x RW) and,
+for batches, the scheduling mode (one persistent launch with one CTA per
+solve, or one tile-queue launch per pass) change speed but never results: every
+candidate runs the same tile routine, so results are bit-identical whatever
+is picked.  The tuner times a short trial of each candidate on the real
+workload (CUDA events, after one warm-up launch) and caches the winner per
+workload signature for the process, optionally in a JSON file named by the
+``WAVEFORGE_B200_TUNE_CACHE`` environment variable.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+from typing import Optional, Sequence
+
+import torch
+
+BATCH_CANDIDATES = (
+    ("persistent", (4, 48, 128, 1, 0)), ("persistent", (6, 48, 128, 1, 0)),
+    ("persistent", (8, 48, 128, 1, 0)), ("tiled", (4, 48, 128, 1, 0)),
+    ("tiled", (6, 48, 128, 1, 0)), ("tiled", (8, 48, 128, 1, 0)),
+    ("tiled", (4, 32, 128, 1, 0)),
+)
+PLAIN_CANDIDATES = ((4, 48, 128, 1, 0), (6, 48, 128, 1, 0), (8, 48, 128, 1, 0),
+                    (4, 32, 64, 1, 0), (4, 32, 128, 1, 0), (2, 32, 64, 1, 0))
+
+_cache: dict = {}
+
+
+def _file() -> Optional[Path]:
+    p = os.environ.get("WAVEFORGE_B200_TUNE_CACHE")
+    return Path(p) if p else None
+
+
+def _load() -> None:
+    f = _file()
+    if f is not None and f.exists() and not _cache.get("_loaded"):
+        try:
+            _cache.update({k: tuple(v) if isinstance(v, list) else v
+                           for k, v in json.loads(f.read_text()).items()})
+        except (OSError, ValueError):
+            pass
+        _cache["_loaded"] = True
+
+
+def _store(key: str, value) -> None:
+    _cache[key] = value
+    f = _file()
+    if f is not None:
+        data = {k: v for k, v in _cache.items() if not k.startswith("_")}
+        f.write_text(json.dumps(data))
+
+
+def batch_signature(solves: Sequence, n_steps: int, device) -> str:
+    shapes: dict = {}
+    for s in solves:
+        key = f"{s.grid.Nx}x{s.grid.Ny}"
+        shapes[key] = shapes.get(key, 0) + 1
+    mat = any(s.Ca is not None for s in solves)
+    name = torch.cuda.get_device_name(device)
+    return f"batch|{name}|{sorted(shapes.items())}|mat={mat}|steps>={min(n_steps, 64)}"
+
+
+def _time(fn, reps: int = 2) -> float:
+    fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def tune_batch(solves: Sequence, n_steps: int, *, device=None, trial_steps: int = 48,
+               candidates=BATCH_CANDIDATES) -> tuple[str, tuple]:
+    """(mode, tune) of the fastest candidate for advancing these solves; each
+    candidate advances every solve ``trial_steps`` steps on scratch copies of
+    the batch's state (the caller's results are untouched)."""
+    from .batch import Batch2D
+    dev = torch.device(device if device is not None else solves[0].grid.device)
+    _load()
+    key = batch_signature(solves, n_steps, dev)
+    if key in _cache:
+        m, t = _cache[key]
+        return m, tuple(t)
+    steps = max(2, min(trial_steps, n_steps))
+    best = None
+    for mode, tune in candidates:
+        b = Batch2D(solves, steps, tune=tune, mode=mode, device=dev)
+
+        def go(b=b):
+            b.reset()
+            b.run()
+        ms = _time(go)
+        if best is None or ms < best[0]:
+            best = (ms, mode, tune)
+        del b
+    _store(key, (best[1], list(best[2])))
+    return best[1], best[2]
+
+
+def tune_plain2d(nx: int, ny: int, *, materials: bool, device, trial_steps: int = 24,
+                 candidates=PLAIN_CANDIDATES) -> tuple:
+    """Fastest (K, tile_i, tile_j, 1, 0) for one nx x ny solve."""
+    from . import _native as nat
+    import ctypes
+    dev = torch.device(device)
+    _load()
+    key = f"plain2d|{torch.cuda.get_device_name(dev)}|{nx}x{ny}|mat={materials}"
+    if key in _cache:
+        return tuple(_cache[key])
+    lib = nat.load()
+    f = torch.zeros((3, nx * ny), dtype=torch.float32, device=dev)
+    s = torch.empty_like(f)
+    c = torch.full((2, nx * ny), 0.5, dtype=torch.float32, device=dev) if materials else None
+    g = nat.WfGrid2D(nx, ny, nat.f32(1e-6), nat.f32(0.1), nat.f32(1e-3), nat.f32(1e-3),
+                     nat.f32(-0.5), nat.f32(-0.5), 0)
+    best = None
+    for t in candidates:
+        tw = nat.WfTune(*t)
+
+        def go(tw=tw):
+            nat.check(lib.wf_fdtd2d_run(
+                ctypes.byref(g), f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(),
+                s[0].data_ptr(), s[1].data_ptr(), s[2].data_ptr(),
+                None if c is None else c[0].data_ptr(), None if c is None else c[1].data_ptr(),
+                None, 0, None, 0, None, 0, 0, 0, trial_steps, 0, None, ctypes.byref(tw),
+                nat.stream_handle(dev)))
+        ms = _time(go)
+        if best is None or ms < best[0]:
+            best = (ms, t)
+    _store(key, list(best[1]))
+    return best[1]

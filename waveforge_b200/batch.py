@@ -145,10 +145,15 @@ class Batch2D:
 
     def __init__(self, solves: Sequence[BatchSolve], n_steps: int, *, tune=None,
                  ctas_per_sm: int = 0, device=None, mode: str = "persistent") -> None:
+        if tune == "auto" or mode == "auto":
+            # time every candidate launch shape on these solves, keep the fastest
+            from .autotune import tune_batch
+            mode, tune = tune_batch(solves, n_steps, device=device)
         if mode not in ("persistent", "tiled"):
-            raise ValueError("mode is 'persistent' (one CTA per solve, one launch) or 'tiled' "
-                             "(one launch per pass over every solve's tiles)")
+            raise ValueError("mode is 'persistent' (one CTA per solve, one launch), 'tiled' "
+                             "(one launch per pass over every solve's tiles) or 'auto'")
         self.mode = mode
+        self._graph = None
         if not solves:
             raise ValueError("Batch2D needs at least one solve")
         self.device = torch.device(device) if device is not None else solves[0].grid.device
@@ -293,6 +298,33 @@ class Batch2D:
                                      None if self.tune is None else ctypes.byref(self.tune),
                                      self.ctas_per_sm, 1 if self._fastdiv else 0,
                                      nat.stream_handle(self.device)))
+
+    def capture(self) -> None:
+        """Record a full run from step 0 (state reset, every launch of the
+        run) in a CUDA graph; ``replay()`` then repeats it with one graph
+        launch.  Descriptors are uploaded once here and stay fixed."""
+        self.reset()
+        self._upload(0, self.n_steps)
+        self.launch()                      # sets kernel attributes before capture
+        torch.cuda.synchronize(self.device)
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(graph, stream=side, capture_error_mode="relaxed"):
+                self._state.zero_()
+                self._traces.zero_()
+                self.launch()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        self._graph = graph
+        self.step = self.n_steps
+
+    def replay(self) -> None:
+        """Re-run the captured run (reset + all steps) on the current stream."""
+        if self._graph is None:
+            raise RuntimeError("capture() first")
+        self._graph.replay()
+        self.step = self.n_steps
 
     def statuses(self) -> list[int]:
         raw = self._desc_dev.cpu().numpy().tobytes()
