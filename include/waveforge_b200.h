@@ -349,6 +349,25 @@ int32_t wf_das2d(const float* traces, const float* traces_ref, int32_t nant, int
                  int32_t gate_start, int32_t skip_self,
                  double* image, void* stream);
 
+/* Travel-time table of AntennaRing.compute_das_image
+ * (src/datasets/brain/antenna.py:216-260, 300-333): tt[a][iy][ix] =
+ * float32 of the one-way time in samples from antenna a (ant_x/y_mm, device)
+ * to pixel (px_mm[ix], py_mm[iy]) (device), through nlayer concentric circles
+ * about (cx_mm, cy_mm) of radius layer_r_mm[l] and permittivity layer_eps[l]
+ * (HOST arrays, outermost first, at most 16; nlayer = 0: free space), c = 3e8. */
+int32_t wf_das_travel_times(int32_t nant, const double* ant_x_mm, const double* ant_y_mm,
+                            const double* px_mm, int32_t nxi, const double* py_mm, int32_t nyi,
+                            double cx_mm, double cy_mm, const double* layer_r_mm,
+                            const double* layer_eps, int32_t nlayer, double dt, float* tt,
+                            void* stream);
+
+/* DAS power image of AntennaRing.compute_das_image (antenna.py:335-341):
+ * image[p] = float32((sum_{tx,rx} env[tx][rx][rint(tt[tx][p] + tt[rx][p])])^2),
+ * samples outside [0, n_steps) skipped, float64 sum in tx-major order.
+ * env: (nant, nant, n_steps) float32 envelope; tt: (nant, npix) float32. */
+int32_t wf_das_envelope_image(const float* env, int32_t nant, int32_t n_steps, const float* tt,
+                              int32_t npix, float* image, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,5 +18,5 @@ from .fdtd_ref import (  # noqa: F401
     EPS0, MU0, C0, stable_dt, material_ca_cb, gauss_deriv_wave, gaussian_wave,
     ricker_wave, Oracle2D, Oracle3D,
 )
-from .das_ref import das_backprojection_ref  # noqa: F401
+from .das_ref import antenna_das_image_ref, das_backprojection_ref  # noqa: F401
 from . import adjoint_ref  # noqa: F401

@@ -419,6 +419,33 @@ def case_das(R, ref: Path, out):
                         tumor=np.array([*ph.tumor_center, ph.tumor_r]))
 
 
+def case_antenna(R, ref: Path, out):
+    """AntennaRing.compute_das_image (src/datasets/brain/antenna.py:262-341) on the
+    breast DAS signals: free-space and layered (ray-circle chord) delays, even and
+    odd trace lengths; the scipy Hilbert envelope is stored for the bit-exact DAS
+    stage."""
+    from scipy.signal import hilbert
+    from datasets.brain.antenna import AntennaRing
+    d = np.load(out / "das_breast96.npz")
+    delta = d["delta"]
+    side = int(d["side"])
+    grid = R["grid"].YeeGrid(side, side, 0.5e-3, 0.5e-3, courant=0.5, device="cpu")
+    GD = gauss_deriv_class(R)
+    res = {}
+    for n_steps in (600, 599):
+        sig = np.ascontiguousarray(delta[:, :, :n_steps])
+        ring = AntennaRing(8, 40, 0, grid)
+        ring.build_sources(GD(), 0, N_steps=n_steps)
+        head = {"cx_cells": 48, "cy_cells": 47, "layers": [(41, 10.0), (33, 5.0), (14, 40.0)]}
+        res[f"img_free_{n_steps}"] = ring.compute_das_image(sig, image_size=40)
+        res[f"img_head_{n_steps}"] = ring.compute_das_image(sig, image_size=33, head_geometry=head)
+        res[f"env_{n_steps}"] = np.abs(hilbert(sig, axis=-1)).astype(np.float32)
+    res["positions"] = np.array(ring.positions)
+    np.savez_compressed(out / "antenna_ring96.npz", dt=grid.dt, dx=grid.dx, side=side,
+                        head_cx=48, head_cy=47, head_layers=np.array([[41, 10.0], [33, 5.0], [14, 40.0]]),
+                        **res)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -436,6 +463,7 @@ def main():
         "head3d": lambda: case_head3d(R, out),
         "edges3d": lambda: case_edges_3d(R, out),
         "das": lambda: case_das(R, ref, out),
+        "antenna": lambda: case_antenna(R, ref, out),
     }
     for k, fn in todo.items():
         if a.only and k not in a.only.split(","):

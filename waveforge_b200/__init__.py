@@ -11,9 +11,10 @@ from .core import *  # noqa: F401,F403
 from .core import __all__ as _core_all
 from .detectors import Detectors
 from .imaging.das import das_backprojection, das_image_device
+from .imaging.antenna import AntennaRing
 from .batch import Batch2D, BatchSolve
 from .adjoint import FDTDMisfit, MisfitProblem2D, fdtd_misfit
 
-__all__ = list(_core_all) + ["Detectors", "das_backprojection", "das_image_device", "Batch2D",
+__all__ = list(_core_all) + ["AntennaRing", "Detectors", "das_backprojection", "das_image_device", "Batch2D",
                              "BatchSolve", "FDTDMisfit", "MisfitProblem2D", "fdtd_misfit"]
 __version__ = "0.1.0"
