@@ -363,7 +363,12 @@ def build_single(args, dev):
         return o, [("Ez",) + tuple(r) for r in wl.receivers()]
 
     name = f"head3d_{n}^3_{wl.steps}steps_{wl.n_rx}rx" + (f"_x{B}_instances" if B > 1 else "")
-    return sim, det, (ca, cb), (cad, cbd), wave, B * n ** 3, 56, make_oracle, name, "k3d_stream"
+    # the library runs the TMA-ring kernel when Nz % 4 == 0 unless a tune picks
+    # the register streaming kernel (variant 1 or 2) or the tile kernel
+    t = _tune_arg(args)
+    kern = ("k3d_tma" if n % 4 == 0 and (t is None or (t[1] == 0 and t[4] == 0))
+            else "k3d_stream" if t is None or t[1] == 0 else "k3d_pass")
+    return sim, det, (ca, cb), (cad, cbd), wave, B * n ** 3, 56, make_oracle, name, kern
 
 
 def cpu_single_sample(make_oracle, cells, max_steps, budget_s=12.0):

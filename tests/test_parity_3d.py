@@ -20,7 +20,7 @@ COMPS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 # None = default (streaming kernel for Nz > 1); tile_i == 0 = streaming with
 # segments of tile_j planes; the rest select the tile kernel
 TUNES3 = [None, (1, 4, 4, 4, 64), (2, 3, 5, 7, 96), (3, 6, 6, 10, 128), (1, 8, 8, 30, 256),
-          (1, 0, 1, 0, 0), (1, 0, 3, 8, 0), (1, 0, 2, 16, 1), (1, 0, 0, 8, 1)]
+          (1, 0, 1, 0, 0), (1, 0, 3, 8, 2), (1, 0, 2, 16, 1), (1, 0, 0, 8, 1), (1, 0, 0, 16, 2)]
 
 
 def sim3d(cuda, shape, dx, courant, srcs, ca=None, cb=None, steps=None, tune=None):
@@ -108,19 +108,21 @@ def test_random_3d_bit_exact_vs_oracle(cuda, seed):
             assert np.array_equal(getattr(f, c).cpu().numpy(), getattr(o, c).numpy()), (tune, c)
 
 
+@pytest.mark.parametrize("tma_shape", [True, False])
 @pytest.mark.parametrize("mat", [False, True])
-def test_streaming_kernel_equals_tile_kernel_multi_block(cuda, mat):
+def test_streaming_kernel_equals_tile_kernel_multi_block(cuda, mat, tma_shape):
     """A volume spanning several 14 x 30 column blocks in j and k and several
     i-segments: the streaming kernel (automatic and forced segment lengths)
     equals the tile kernel bit for bit in traces, final fields and the
     stability maxima, with E and H sources inside and across block edges."""
     rng = np.random.default_rng(77 + mat)
-    shape = (23, 37, 71)
+    shape = (23, 37, 72) if tma_shape else (23, 37, 71)
     nx, ny, nz = shape
     steps = 17
     srcs = []
     for c, (i, j, k) in (("Ez", (11, 14, 30)), ("Hy", (5, 15, 31)), ("Ex", (0, 0, 0)),
-                         ("Hx", (22, 36, 70)), ("Ey", (12, 28, 59))):
+                         ("Hx", (22, 36, nz - 1)), ("Ey", (12, 28, 59)), ("Ez", (20, 13, 29)),
+                         ("Ex", (3, 27, 60))):
         srcs.append((c, (i, i + 1, j, j + 1, k, k + 1),
                      torch.from_numpy(rng.standard_normal(steps).astype(np.float32))))
     ca = cb = None
@@ -129,10 +131,10 @@ def test_streaming_kernel_equals_tile_kernel_multi_block(cuda, mat):
         cb = torch.from_numpy(rng.uniform(0.001, 0.1, shape).astype(np.float32))
     probes = [(COMPS[q % 6], int(rng.integers(0, nx)), int(rng.integers(0, ny)),
                int(rng.integers(0, nz))) for q in range(24)]
-    probes += [("Hx", 0, 14, 30), ("Hz", 22, 0, 0), ("Ey", 11, 15, 29), ("Hy", 3, 36, 70)]
+    probes += [("Hx", 0, 14, 30), ("Hz", 22, 0, 0), ("Ey", 11, 15, 29), ("Hy", 3, 36, nz - 1)]
     outs = []
-    for tune in ((1, 8, 8, 30, 256), None, (1, 0, 2, 0, 0), (1, 0, 7, 8, 0), (1, 0, 5, 16, 1),
-                 (1, 0, 0, 8, 1)):
+    for tune in ((1, 8, 8, 30, 256), None, (1, 0, 2, 0, 0), (1, 0, 7, 8, 2), (1, 0, 5, 16, 1),
+                 (1, 0, 0, 8, 1), (1, 0, 0, 16, 2), (1, 0, 1, 0, 0)):
         sim, f = sim3d(cuda, shape, 1e-3, 0.9, srcs, ca, cb, steps=steps, tune=tune)
         sim._n_check = 4
         tr = sim.run(steps, record=Detectors(probes))

@@ -734,6 +734,75 @@ static int launch_stream_cfg(const Tile3D& P, int seg_len, int n, int nb, cudaSt
   return WF_OK;
 }
 
+}  // namespace wf
+
+#include "fdtd3d_tma.cuh"
+
+namespace wf {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+typedef CUresult (*TmaEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static TmaEncodeFn tma_encoder() {
+  static TmaEncodeFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<TmaEncodeFn>(ptr);
+  }
+  return fn;
+}
+
+// 4D map {k, j, i, instance} of one float32 array with a kBoxK x kTJ x 1 x 1
+// box; false when the layout breaks a TMA rule (16-byte strides / base).
+static bool tma_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, int ninst,
+                    long long istride) {
+  TmaEncodeFn fn = tma_encoder();
+  if (fn == nullptr || base == nullptr || (nz & 3) || (reinterpret_cast<uintptr_t>(base) & 15) ||
+      (ninst > 1 && (istride & 3)))
+    return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx, (cuuint64_t)ninst};
+  const long long plane = (long long)nx * ny * nz;
+  const cuuint64_t strides[3] = {(cuuint64_t)nz * 4, (cuuint64_t)ny * nz * 4,
+                                 (cuuint64_t)(ninst > 1 ? istride : plane) * 4};
+  const cuuint32_t box[4] = {(cuuint32_t)kBoxK, (cuuint32_t)kTJ, 1, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box,
+            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <bool MAT, bool FDIV>
+static int launch_tma(const TmaMaps& maps, const Tile3D& P, int seg_len, int n, int nb,
+                      cudaStream_t st) {
+  const int tiles_j = (P.ny + kTCJ - 1) / kTCJ, tiles_k = (P.nz + kTCK - 1) / kTCK;
+  const int nseg = (P.nx + seg_len - 1) / seg_len;
+  const long long nblk = (long long)tiles_j * tiles_k * nseg;
+  if (nblk > 0x7fffffffLL || nb < 1 || nb > 65535)
+    return set_error(WF_E_LIMIT, "wf_fdtd3d: too many column blocks or instances");
+  const size_t smem = sizeof(TmaSmem);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k3d_tma<MAT, FDIV>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k3d_tma)");
+    attr = true;
+  }
+  dim3 grid((unsigned)nblk, (unsigned)nb);
+  k3d_tma<MAT, FDIV><<<grid, kTJ * kTK, smem, st>>>(maps, P, tiles_j, tiles_k, seg_len, n, nullptr);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "launch k3d_tma");
+  return WF_OK;
+}
+
 // Streaming variants: rows per column block (16 = 512 threads, one CTA per
 // SM; 8 = 256 threads, two per SM) and whether the Faraday update reads its
 // j neighbour directly (no shared exchange, one CTA barrier less per plane).
@@ -756,6 +825,19 @@ static int stream_seg_len(int nx, int ny, int nz, int rows) {
   const long long plane = (long long)((ny + rows - 3) / (rows - 2)) * ((nz + kCK - 1) / kCK);
   long long nseg = (4LL * nsm + plane - 1) / plane;
   nseg = std::max(1LL, std::min(nseg, (long long)std::max(1, nx / 8)));
+  return (int)((nx + nseg - 1) / nseg);
+}
+
+// Segment length of the TMA kernel: about one wave of resident CTAs (two per
+// SM) over all instances, at least 16 planes per segment (each segment
+// re-reads three planes).
+static int tma_seg_len(int nx, int ny, int nz, int nb) {
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long cols = (long long)((ny + kTCJ - 1) / kTCJ) * ((nz + kTCK - 1) / kTCK) * nb;
+  long long nseg = (2LL * nsm + cols - 1) / cols;
+  nseg = std::max(1LL, std::min(nseg, (long long)std::max(1, nx / 16)));
   return (int)((nx + nseg - 1) / nseg);
 }
 
@@ -792,14 +874,17 @@ static int run3d(const wf_grid3d* g, int nb, long long fstride, long long cstrid
   wf_tune t{};
   bool stream_k = false, direct = true;
   int seg_len = 0, rows = 16;
+  int variant = 0;  // streaming: 0 = TMA ring when the layout allows, else 2
   if (tune && tune->tile_i == 0) {
-    // streaming: tile_j = segment length (0 = automatic), tile_k = rows per
-    // column block (8 or 16; 0 = 16), threads = 1 for the shared-memory
-    // j exchange instead of direct neighbour loads
+    // streaming: tile_j = segment length (0 = automatic); threads selects the
+    // variant: 0 TMA ring (register kernel when Nz % 4 != 0), 1 register
+    // kernel with shared j exchange, 2 register kernel with direct j loads;
+    // tile_k = rows per column block of the register kernel (8 or 16)
     stream_k = true;
     seg_len = tune->tile_j;
     rows = tune->tile_k == 8 ? 8 : 16;
-    direct = tune->threads != 1;
+    variant = tune->threads;
+    direct = variant != 1;
     if (seg_len < 0) return set_error(WF_E_ARG, "wf_fdtd3d_run: negative segment length");
   } else if (tune) {
     t = *tune;
@@ -814,9 +899,10 @@ static int run3d(const wf_grid3d* g, int nb, long long fstride, long long cstrid
   }
   if (nb > 1 && !stream_k)
     return set_error(WF_E_ARG, "wf_fdtd3d_batch_run: batched instances need the streaming kernel");
+  const bool auto_seg = seg_len == 0;
   if (stream_k) {
     t.steps_per_pass = 1;
-    if (seg_len == 0) seg_len = stream_seg_len(g->nx, g->ny, g->nz, rows);
+    if (auto_seg) seg_len = stream_seg_len(g->nx, g->ny, g->nz, rows);
   } else if (t.steps_per_pass < 1 || t.steps_per_pass > 8 || t.tile_i < 2 || t.tile_j < 2 ||
              t.tile_k < 2 || t.threads < 32 || t.threads > 512 || (t.threads & 31)) {
     return set_error(WF_E_ARG, "wf_fdtd3d_run: bad tune");
@@ -853,6 +939,21 @@ static int run3d(const wf_grid3d* g, int nb, long long fstride, long long cstrid
   const int all3 = WF_FASTDIV_X | WF_FASTDIV_Y | WF_FASTDIV_Z;
   const int all2 = WF_FASTDIV_X | WF_FASTDIV_Y;
   const bool fd = g->nz > 1 ? (g->flags & all3) == all3 : (g->flags & all2) == all2;
+  // TMA tensor maps of both ping-pong sets (and Ca/Cb), encoded once per call
+  TmaMaps mapsA{}, mapsB{};
+  bool tma = stream_k && variant == 0;
+  if (tma) {
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    for (int c = 0; c < 6 && tma; ++c)
+      tma = tma_map(&mapsA.m[c], f[c], nx, ny, nz, nb, fstride) &&
+            tma_map(&mapsB.m[c], s[c], nx, ny, nz, nb, fstride);
+    if (tma && ca)
+      tma = tma_map(&mapsA.m[6], ca, nx, ny, nz, cstride ? nb : 1, cstride) &&
+            tma_map(&mapsA.m[7], cb, nx, ny, nz, cstride ? nb : 1, cstride);
+    mapsB.m[6] = mapsA.m[6];
+    mapsB.m[7] = mapsA.m[7];
+    if (tma && auto_seg) seg_len = tma_seg_len(g->nx, g->ny, g->nz, nb);
+  }
   const PassPlan plan(nsteps, t.steps_per_pass);
   for (int p = 0; p < plan.passes(); ++p) {
     float* const* in = (p & 1) ? s : f;
@@ -863,7 +964,13 @@ static int run3d(const wf_grid3d* g, int nb, long long fstride, long long cstrid
     }
     const int s0 = step0 + plan.offset(p), k = plan.len(p);
     int rc;
-    if (stream_k)
+    if (tma) {
+      const TmaMaps& m = (p & 1) ? mapsB : mapsA;
+      rc = ca ? (fd ? launch_tma<true, true>(m, P, seg_len, s0, nb, st)
+                    : launch_tma<true, false>(m, P, seg_len, s0, nb, st))
+              : (fd ? launch_tma<false, true>(m, P, seg_len, s0, nb, st)
+                    : launch_tma<false, false>(m, P, seg_len, s0, nb, st));
+    } else if (stream_k)
       rc = ca ? (fd ? launch_stream<true, true>(P, seg_len, s0, rows, direct, nb, st)
                     : launch_stream<true, false>(P, seg_len, s0, rows, direct, nb, st))
               : (fd ? launch_stream<false, true>(P, seg_len, s0, rows, direct, nb, st)

@@ -1,0 +1,362 @@
+// fdtd3d_tma.cuh -- k3d_tma: the single-step 3D streaming pass with its
+// i-planes staged in shared memory by the Tensor Memory Accelerator.
+// Included by fdtd3d.cu (uses Tile3D, Lists3D, dv<>, src3_value).
+//
+// A CTA owns a 16 (j) x 32 (k) block of columns -- a 14 x 30 core with a
+// one-cell halo -- and walks an i-segment exactly like k3d_stream, with the
+// same float ops in the same order (so the two are bit-identical).  What
+// changes is data movement: one thread issues, per i-plane, one
+// cp.async.bulk.tensor load per array (Ex, Ey, Ez, Hx, Hy, Hz and Ca, Cb) of a
+// 16 x 36 box into a 4-slot shared-memory ring, completing on the slot's
+// mbarrier; plane f+3 is in flight while plane f is finished.  All
+// neighbours (j +- 1, k +- 1, i +- 1) are read from shared memory, so no
+// thread issues global loads, shuffles or address arithmetic for them.  The
+// box starts at k = floor4(k0 - 1) (a TMA box must start on a 16-byte
+// boundary); lanes read column lane + (k0 - 1 - floor4(k0 - 1)).
+// Curl-updated H of planes f-1..f+1 and the final H of plane f live in shared
+// rows for the Mur faces and the Ampere neighbours.  Every mbarrier wait is
+// bounded: after the limit the CTA records WF_E_TIMEOUT and stops.
+#pragma once
+
+#include <cuda.h>
+
+namespace wf {
+
+constexpr int kTJ = 16, kTK = 32, kTCJ = kTJ - 2, kTCK = kTK - 2;
+constexpr int kBoxK = 36;                       // box width in k (>= 32 + 3 + 1)
+constexpr int kRing = 4;                        // i-plane slots
+constexpr int kTileF = kTJ * kBoxK;             // floats per array per slot
+constexpr unsigned kSpinLimit = 1u << 22;       // bounded mbarrier wait
+
+struct TmaMaps {
+  CUtensorMap m[8];  // Ex, Ey, Ez, Hx, Hy, Hz (pass input), Ca, Cb
+};
+
+struct TmaSmem {
+  float raw[kRing][8][kTJ][kBoxK];  // slot, array, row, column
+  float hc[3][3][kTJ][kTK];         // curl-updated H of planes (p mod 3)
+  float hf[3][kTJ][kTK];            // final H of plane f
+  float hom[2][kTJ][kTK];           // old Hy, Hz of plane Nx-2 (x face at Nx-1)
+  unsigned long long bar[kRing];
+  Lists3D L;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// One 4D tile load {k, j, i, instance} into shared memory, completing on b.
+__device__ __forceinline__ void tma_load4(void* dst, const CUtensorMap* map, int c0, int c1,
+                                          int c2, int c3, unsigned long long* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(smem_u32(b))
+      : "memory");
+}
+
+template <bool MAT, bool FDIV>
+__global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ TmaMaps maps,
+                                                        Tile3D P, int tiles_j, int tiles_k,
+                                                        int seg_len, int n, int* status) {
+  extern __shared__ __align__(128) unsigned char smraw3[];
+  TmaSmem& S = *reinterpret_cast<TmaSmem*>(smraw3);
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  int b = blockIdx.x;
+  const int tk = b % tiles_k;
+  b /= tiles_k;
+  const int tj = b % tiles_j, seg = b / tiles_j;
+  const int inst = blockIdx.y;
+  if (inst) {
+    const long long q = inst;
+    for (int c = 0; c < 6; ++c) P.out[c] += q * P.fstride;
+    P.traces += q * P.tstride;
+    P.src += q * P.sstride;
+  }
+  const int ci_inst = P.cstride ? inst : 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, tid = threadIdx.x;
+  const int j0 = tj * kTCJ - 1, k0 = tk * kTCK - 1;  // region origin (halo included)
+  const int kb = k0 >= 0 ? (k0 & ~3) : -(((-k0) + 3) & ~3);  // floor to a multiple of 4
+  const int cofs = k0 - kb;                                   // 0..3
+  const int gj = j0 + w, gk = k0 + lane;
+  const bool in = gj >= 0 && gj < ny && gk >= 0 && gk < nz;
+  const bool core = in && w >= 1 && w <= kTCJ && lane >= 1 && lane <= kTCK;
+  const int col = lane + cofs;
+  const int ia = seg * seg_len, ib = min(nx, ia + seg_len);
+  if (ia >= ib) return;
+  const int f0 = max(ia - 1, 0);
+  const int plast = min(nx - 1, ib + 1);  // last plane the segment reads
+  const long long PS = (long long)ny * nz;
+  const long long colg = in ? (long long)gj * nz + gk : 0;
+  const float dh = P.dh, de = P.de, dx = P.dx, dy = P.dy, dz = P.dz;
+  const float mx = P.mx, my = P.my, mz = P.mz;
+  const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy),
+               rdz = __drcp_rn((double)dz);
+  const int narr = MAT ? 8 : 6;
+  const unsigned bytes = (unsigned)(narr * kTileF * sizeof(float));
+
+  if (tid == 0) {
+    for (int s = 0; s < kRing; ++s) mbar_init(&S.bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    int nh = 0, ne = 0;
+    for (int q = 0; q < P.nsrc; ++q) {
+      const wf_source& Q = P.src[q];
+      if (Q.i1 <= f0 || Q.i0 > plast || Q.j1 <= j0 || Q.j0 >= j0 + kTJ || Q.k1 <= k0 ||
+          Q.k0 >= k0 + kTK)
+        continue;
+      if (Q.comp >= WF_HX) {
+        if (nh < kMaxLocalSrc3) S.L.h[nh++] = (short)q;
+      } else {
+        if (ne < kMaxLocalSrc3) S.L.e[ne++] = (short)q;
+      }
+    }
+    S.L.nh = nh;
+    S.L.ne = ne;
+    S.L.np = 0;
+    for (int c = 0; c < 6; ++c) S.L.bmax[c] = 0u;
+  }
+  __syncthreads();
+  for (int q = tid; q < P.nprb; q += blockDim.x) {
+    const wf_probe& pr = P.prb[q];
+    if (pr.i >= ia && pr.i < ib && pr.j >= j0 + 1 && pr.j < j0 + 1 + kTCJ && pr.k >= k0 + 1 &&
+        pr.k < k0 + 1 + kTCK) {
+      const int slot = atomicAdd(&S.L.np, 1);
+      if (slot < kMaxLocalProbe3) S.L.p[slot] = (short)q;
+    }
+  }
+  const int ne = S.L.ne, nh = S.L.nh;
+
+  auto issue = [&](int p) {  // thread 0 only
+    const int s = p % kRing;
+    // the slot may hold source values written by ordinary stores: order them
+    // before the asynchronous-proxy overwrite
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&S.bar[s], bytes);
+    for (int c = 0; c < 6; ++c) tma_load4(&S.raw[s][c][0][0], &maps.m[c], kb, j0, p, inst, &S.bar[s]);
+    if (MAT) {
+      tma_load4(&S.raw[s][6][0][0], &maps.m[6], kb, j0, p, ci_inst, &S.bar[s]);
+      tma_load4(&S.raw[s][7][0][0], &maps.m[7], kb, j0, p, ci_inst, &S.bar[s]);
+    }
+  };
+  unsigned phase = 0u;  // parity bit per slot
+  bool failed = false;
+  // Wait for plane p, then add this CTA's E-source values into it (each
+  // column-owner adds to its own cell).
+  auto land = [&](int p) {
+    const int s = p % kRing;
+    const unsigned par = (phase >> s) & 1u;
+    unsigned spin = 0;
+    while (!failed && !mbar_try_wait(&S.bar[s], par)) {
+      if (++spin > kSpinLimit) {
+        failed = true;
+        if (status != nullptr) atomicExch(status, WF_E_TIMEOUT);
+      }
+    }
+    phase ^= 1u << s;
+    if (ne > 0 && in) {
+      for (int q = 0; q < ne; ++q) {
+        const wf_source& Q = P.src[S.L.e[q]];
+        if (p >= Q.i0 && p < Q.i1 && gj >= Q.j0 && gj < Q.j1 && gk >= Q.k0 && gk < Q.k1) {
+          const float v = src3_value(Q, p, gj, gk, n);
+          float& cell = S.raw[s][Q.comp][w][col];
+          cell = fadd(cell, v);
+        }
+      }
+    }
+  };
+
+  // Faraday update of plane p into S.hc[p % 3] (all region cells).
+  auto curl = [&](int p) {
+    const int s = p % kRing, s1 = (p + 1) % kRing, h = p % 3;
+    const float ex = S.raw[s][0][w][col], ey = S.raw[s][1][w][col], ez = S.raw[s][2][w][col];
+    const bool jn = w + 1 < kTJ;
+    const float ex_j = jn ? S.raw[s][0][w + 1][col] : 0.f;
+    const float ez_j = jn ? S.raw[s][2][w + 1][col] : 0.f;
+    const float ex_k = S.raw[s][0][w][col + 1], ey_k = S.raw[s][1][w][col + 1];
+    const bool inext = p + 1 < nx;
+    const float ey_i = inext ? S.raw[s1][1][w][col] : 0.f;
+    const float ez_i = inext ? S.raw[s1][2][w][col] : 0.f;
+    float vx = S.raw[s][3][w][col], vy = S.raw[s][4][w][col], vz = S.raw[s][5][w][col];
+    for (int q = 0; q < nh; ++q) {
+      const wf_source& Q = P.src[S.L.h[q]];
+      if (p >= Q.i0 && p < Q.i1 && gj >= Q.j0 && gj < Q.j1 && gk >= Q.k0 && gk < Q.k1) {
+        const float v = src3_value(Q, p, gj, gk, n);
+        if (Q.comp == WF_HX) vx = fadd(vx, v);
+        else if (Q.comp == WF_HY) vy = fadd(vy, v);
+        else vz = fadd(vz, v);
+      }
+    }
+    if (gj < ny - 1 && gk < nz - 1) {
+      const float t1 = dv<FDIV>(fsub(ey_k, ey), dz, rdz);
+      const float t2 = dv<FDIV>(fsub(ez_j, ez), dy, rdy);
+      vx = fadd(vx, fmul(dh, fsub(t1, t2)));
+    }
+    if (p < nx - 1 && gk < nz - 1) {
+      const float t1 = dv<FDIV>(fsub(ez_i, ez), dx, rdx);
+      const float t2 = dv<FDIV>(fsub(ex_k, ex), dz, rdz);
+      vy = fadd(vy, fmul(dh, fsub(t1, t2)));
+    }
+    if (p < nx - 1 && gj < ny - 1) {
+      const float t1 = dv<FDIV>(fsub(ex_j, ex), dy, rdy);
+      const float t2 = dv<FDIV>(fsub(ey_i, ey), dx, rdx);
+      vz = fadd(vz, fmul(dh, fsub(t1, t2)));
+    }
+    S.hc[h][0][w][lane] = vx;
+    S.hc[h][1][w][lane] = vy;
+    S.hc[h][2][w][lane] = vz;
+  };
+
+  // ---- prologue ---------------------------------------------------------------
+  if (tid == 0) {
+    for (int p = f0; p <= min(f0 + 2, plast); ++p) issue(p);
+  }
+  land(f0);
+  if (f0 + 1 <= plast) land(f0 + 1);
+  failed = __syncthreads_or(failed) != 0;
+  if (!failed) curl(f0);
+  F3 hprev{0.f, 0.f, 0.f};
+  unsigned mxb[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+  const bool check = P.check_max != nullptr && P.n_check > 0 && (n + 1) % P.n_check == 0;
+  const bool zf_on = nz > 1;
+
+  for (int f = f0; f < ib && !failed; ++f) {
+    const int p = f + 1;
+    if (f + 2 <= plast) land(f + 2);
+    // A: slot of plane f-1 is free; injections and hc(f) visible; a timed-out
+    // wait anywhere stops the whole CTA
+    failed = __syncthreads_or(failed) != 0;
+    if (failed) break;
+    if (tid == 0 && f + 3 <= plast) issue(f + 3);
+    if (p < nx) curl(p);
+    __syncthreads();  // B: hc(p) visible
+    // ---- Mur faces of plane f, as pure functions of old and curl-updated H ----
+    const int sf = f % kRing, sp = p % kRing, hf0 = f % 3, hp = p % 3, hm = (f + 2) % 3;
+    auto Ho = [&](int c, int ww, int ll) -> float { return S.raw[sf][3 + c][ww][ll + cofs]; };
+    auto Hc = [&](int c, int ww, int ll) -> float { return S.hc[hf0][c][ww][ll]; };
+    // Hy, Hz after the x faces
+    auto xf = [&](int c, int ww, int ll) -> float {
+      if (f == 0) return fadd(S.raw[sp][3 + c][ww][ll + cofs],
+                              fmul(mx, fsub(S.hc[hp][c][ww][ll], Ho(c, ww, ll))));
+      if (f == nx - 1) return fadd(S.hom[c - 1][ww][ll], fmul(mx, fsub(S.hc[hm][c][ww][ll], Ho(c, ww, ll))));
+      return Hc(c, ww, ll);
+    };
+    // Hx after the y faces (Hx has no x face)
+    auto yfx = [&](int ww, int ll) -> float {
+      const int g = j0 + ww;
+      if (g == 0 && ww + 1 < kTJ) return fadd(Ho(0, ww + 1, ll), fmul(my, fsub(Hc(0, ww + 1, ll), Ho(0, ww, ll))));
+      if (g == ny - 1 && ww >= 1) return fadd(Ho(0, ww - 1, ll), fmul(my, fsub(Hc(0, ww - 1, ll), Ho(0, ww, ll))));
+      return Hc(0, ww, ll);
+    };
+    float hxF = yfx(w, lane), hyF = xf(1, w, lane), hzF = xf(2, w, lane);
+    if (gj == 0 && w + 1 < kTJ)
+      hzF = fadd(Ho(2, w + 1, lane), fmul(my, fsub(xf(2, w + 1, lane), Ho(2, w, lane))));
+    else if (gj == ny - 1 && w >= 1)
+      hzF = fadd(Ho(2, w - 1, lane), fmul(my, fsub(xf(2, w - 1, lane), Ho(2, w, lane))));
+    if (zf_on && in) {
+      if (gk == 0 && lane + 1 < kTK) {
+        hxF = fadd(Ho(0, w, lane + 1), fmul(mz, fsub(yfx(w, lane + 1), Ho(0, w, lane))));
+        hyF = fadd(Ho(1, w, lane + 1), fmul(mz, fsub(xf(1, w, lane + 1), Ho(1, w, lane))));
+      } else if (gk == nz - 1 && lane >= 1) {
+        hxF = fadd(Ho(0, w, lane - 1), fmul(mz, fsub(yfx(w, lane - 1), Ho(0, w, lane))));
+        hyF = fadd(Ho(1, w, lane - 1), fmul(mz, fsub(xf(1, w, lane - 1), Ho(1, w, lane))));
+      }
+    }
+    S.hf[0][w][lane] = hxF;
+    S.hf[1][w][lane] = hyF;
+    S.hf[2][w][lane] = hzF;
+    if (f == nx - 2) {
+      S.hom[0][w][lane] = Ho(1, w, lane);
+      S.hom[1][w][lane] = Ho(2, w, lane);
+    }
+    __syncthreads();  // C: final H of plane f visible
+    // ---- Ampere update and outputs of plane f ----
+    if (f >= ia && core) {
+      const float hz_j = S.hf[2][w - 1][lane], hx_j = S.hf[0][w - 1][lane];
+      const float hy_k = S.hf[1][w][lane - 1], hx_k = S.hf[0][w][lane - 1];
+      float ex = S.raw[sf][0][w][col], ey = S.raw[sf][1][w][col], ez = S.raw[sf][2][w][col];
+      const float cav = MAT ? S.raw[sf][6][w][col] : 0.f, cbv = MAT ? S.raw[sf][7][w][col] : 0.f;
+      if (gj >= 1 && gk >= 1) {
+        const float c = fsub(dv<FDIV>(fsub(hzF, hz_j), dy, rdy), dv<FDIV>(fsub(hyF, hy_k), dz, rdz));
+        ex = MAT ? fadd(fmul(cav, ex), fmul(cbv, c)) : fadd(ex, fmul(de, c));
+      }
+      if (f >= 1 && gk >= 1) {
+        const float c = fsub(dv<FDIV>(fsub(hxF, hx_k), dz, rdz), dv<FDIV>(fsub(hzF, hprev.z), dx, rdx));
+        ey = MAT ? fadd(fmul(cav, ey), fmul(cbv, c)) : fadd(ey, fmul(de, c));
+      }
+      if (f >= 1 && gj >= 1) {
+        const float c = fsub(dv<FDIV>(fsub(hyF, hprev.y), dx, rdx), dv<FDIV>(fsub(hxF, hx_j), dy, rdy));
+        ez = MAT ? fadd(fmul(cav, ez), fmul(cbv, c)) : fadd(ez, fmul(de, c));
+      }
+      const long long o = (long long)f * PS + colg;
+      P.out[0][o] = ex;
+      P.out[1][o] = ey;
+      P.out[2][o] = ez;
+      P.out[3][o] = hxF;
+      P.out[4][o] = hyF;
+      P.out[5][o] = hzF;
+      const int np = min(S.L.np, kMaxLocalProbe3);
+      for (int q = 0; q < np; ++q) {
+        const wf_probe& pr = P.prb[S.L.p[q]];
+        if (pr.i == f && pr.j == gj && pr.k == gk) {
+          const float v = pr.comp == WF_EX ? ex : pr.comp == WF_EY ? ey : pr.comp == WF_EZ ? ez
+                        : pr.comp == WF_HX ? hxF : pr.comp == WF_HY ? hyF : hzF;
+          P.traces[(long long)S.L.p[q] * P.trace_ld + (n - P.trace_step0)] = v;
+        }
+      }
+      if (check) {
+        mxb[0] = max(mxb[0], abs_bits(ex));
+        mxb[1] = max(mxb[1], abs_bits(ey));
+        mxb[2] = max(mxb[2], abs_bits(ez));
+        mxb[3] = max(mxb[3], abs_bits(hxF));
+        mxb[4] = max(mxb[4], abs_bits(hyF));
+        mxb[5] = max(mxb[5], abs_bits(hzF));
+      }
+    }
+    hprev = F3{hxF, hyF, hzF};
+  }
+  // every issued plane has been waited on (planes up to plast are landed in
+  // the loop); a failed wait leaves copies in flight: wait them out, bounded
+  if (failed && tid == 0) {
+    for (int s = 0; s < kRing; ++s) {
+      unsigned spin = 0;
+      while (!mbar_try_wait(&S.bar[s], (phase >> s) & 1u) && ++spin < kSpinLimit) {
+      }
+    }
+  }
+  if (check) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      for (int sh = 16; sh > 0; sh >>= 1) mxb[c] = max(mxb[c], __shfl_xor_sync(0xffffffffu, mxb[c], sh));
+      if (lane == 0) atomicMax(&S.L.bmax[c], mxb[c]);
+    }
+    __syncthreads();
+    if (tid < 6) {
+      const int idx = (n + 1) / P.n_check - P.check_base - 1;
+      atomicMax(&P.check_max[idx * 6 + tid], S.L.bmax[tid]);
+    }
+  }
+}
+
+}  // namespace wf
