@@ -780,6 +780,20 @@ static bool tma_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, i
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Opt k3d_tma into its dynamic shared memory (once per instantiation).
+template <bool MAT, bool FDIV>
+static int tma_attr() {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k3d_tma<MAT, FDIV>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(TmaSmem));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k3d_tma)");
+    attr = true;
+  }
+  return WF_OK;
+}
+
 template <bool MAT, bool FDIV>
 static int launch_tma(const TmaMaps& maps, const Tile3D& P, int seg_len, int n, int nb,
                       cudaStream_t st) {
@@ -789,13 +803,8 @@ static int launch_tma(const TmaMaps& maps, const Tile3D& P, int seg_len, int n, 
   if (nblk > 0x7fffffffLL || nb < 1 || nb > 65535)
     return set_error(WF_E_LIMIT, "wf_fdtd3d: too many column blocks or instances");
   const size_t smem = sizeof(TmaSmem);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k3d_tma<MAT, FDIV>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k3d_tma)");
-    attr = true;
-  }
+  const int rc = tma_attr<MAT, FDIV>();
+  if (rc != WF_OK) return rc;
   dim3 grid((unsigned)nblk, (unsigned)nb);
   k3d_tma<MAT, FDIV><<<grid, kTJ * kTK, smem, st>>>(maps, P, tiles_j, tiles_k, seg_len, n, nullptr);
   cudaError_t e = cudaGetLastError();
@@ -828,17 +837,36 @@ static int stream_seg_len(int nx, int ny, int nz, int rows) {
   return (int)((nx + nseg - 1) / nseg);
 }
 
-// Segment length of the TMA kernel: about one wave of resident CTAs (two per
-// SM) over all instances, at least 16 planes per segment (each segment
-// re-reads three planes).
+// Segment length of the TMA kernel.  A column block costs about (planes + 2)
+// plane-steps (each segment re-reads three planes, mostly from L2); a launch
+// takes the total spread over the resident slots plus about one block's
+// length of tail.  Pick the segment count that minimises
+// blocks x (L + 2) / slots + (L + 2), with at least 16 planes per segment
+// (on 256^3 and 8 x 128^3 volumes this picks the best length of a sweep).
+template <bool MAT, bool FDIV>
 static int tma_seg_len(int nx, int ny, int nz, int nb) {
-  int dev = 0, nsm = 148;
+  int dev = 0, nsm = 148, per_sm = 2;
   if (cudaGetDevice(&dev) == cudaSuccess)
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (tma_attr<MAT, FDIV>() != WF_OK ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3d_tma<MAT, FDIV>, kTJ * kTK,
+                                                    sizeof(TmaSmem)) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const long long slots = (long long)nsm * per_sm;
   const long long cols = (long long)((ny + kTCJ - 1) / kTCJ) * ((nz + kTCK - 1) / kTCK) * nb;
-  long long nseg = (2LL * nsm + cols - 1) / cols;
-  nseg = std::max(1LL, std::min(nseg, (long long)std::max(1, nx / 16)));
-  return (int)((nx + nseg - 1) / nseg);
+  const int max_seg = std::max(1, nx / 16);
+  int best = 1;
+  long long best_cost = -1;
+  for (int ns = 1; ns <= max_seg; ++ns) {
+    const long long len = (nx + ns - 1) / ns;
+    const long long cost = cols * ns * (len + 2) + slots * (len + 2);  // x slots
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = ns;
+    }
+  }
+  return (nx + best - 1) / best;
 }
 
 }  // namespace wf
@@ -952,7 +980,11 @@ static int run3d(const wf_grid3d* g, int nb, long long fstride, long long cstrid
             tma_map(&mapsA.m[7], cb, nx, ny, nz, cstride ? nb : 1, cstride);
     mapsB.m[6] = mapsA.m[6];
     mapsB.m[7] = mapsA.m[7];
-    if (tma && auto_seg) seg_len = tma_seg_len(g->nx, g->ny, g->nz, nb);
+    if (tma && auto_seg)
+      seg_len = ca ? (fd ? tma_seg_len<true, true>(g->nx, g->ny, g->nz, nb)
+                         : tma_seg_len<true, false>(g->nx, g->ny, g->nz, nb))
+                   : (fd ? tma_seg_len<false, true>(g->nx, g->ny, g->nz, nb)
+                         : tma_seg_len<false, false>(g->nx, g->ny, g->nz, nb));
   }
   const PassPlan plan(nsteps, t.steps_per_pass);
   for (int p = 0; p < plan.passes(); ++p) {

@@ -26,6 +26,9 @@ constexpr int kTJ = 16, kTK = 32, kTCJ = kTJ - 2, kTCK = kTK - 2;
 constexpr int kBoxK = 36;                       // box width in k (>= 32 + 3 + 1)
 constexpr int kRing = 4;                        // i-plane slots
 constexpr int kTileF = kTJ * kBoxK;             // floats per array per slot
+constexpr int kSlotF = 8 * kTileF;              // floats per slot
+constexpr int kHcF = kTJ * kTK;                 // floats per H row set component
+constexpr int kHcSetF = 3 * kHcF;               // floats per plane of hc
 constexpr unsigned kSpinLimit = 1u << 22;       // bounded mbarrier wait
 
 struct TmaMaps {
@@ -187,18 +190,33 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     }
   };
 
-  // Faraday update of plane p into S.hc[p % 3] (all region cells).
-  auto curl = [&](int p) {
-    const int s = p % kRing, s1 = (p + 1) % kRing, h = p % 3;
-    const float ex = S.raw[s][0][w][col], ey = S.raw[s][1][w][col], ez = S.raw[s][2][w][col];
-    const bool jn = w + 1 < kTJ;
-    const float ex_j = jn ? S.raw[s][0][w + 1][col] : 0.f;
-    const float ez_j = jn ? S.raw[s][2][w + 1][col] : 0.f;
-    const float ex_k = S.raw[s][0][w][col + 1], ey_k = S.raw[s][1][w][col + 1];
-    const bool inext = p + 1 < nx;
-    const float ey_i = inext ? S.raw[s1][1][w][col] : 0.f;
-    const float ez_i = inext ? S.raw[s1][2][w][col] : 0.f;
-    float vx = S.raw[s][3][w][col], vy = S.raw[s][4][w][col], vz = S.raw[s][5][w][col];
+  // Per-thread shared-memory bases: slot arrays are addressed as
+  // R[c * kTileF] (+ kBoxK for j + 1, + 1 for k + 1), H rows as Hrow[c * kHcF].
+  float* const raw0 = &S.raw[0][0][0][0] + (w * kBoxK + col);
+  float* const hc0 = &S.hc[0][0][0][0] + (w * kTK + lane);
+  const bool cjk = gj < ny - 1 && gk < nz - 1, ck = gk < nz - 1, cj = gj < ny - 1;
+  // a block none of whose cells lies on a j or k face needs the Mur code only
+  // on the planes i = 0 and i = Nx - 1
+  const bool face_blk = !(j0 >= 1 && j0 + kTJ - 1 <= ny - 2 && k0 >= 1 && k0 + kTK - 1 <= nz - 2);
+  // carried between planes: Ey, Ez of plane p (read as the i + 1 neighbours
+  // of plane p - 1), E of the plane being finished, curl-updated H
+  float cey = 0.f, cez = 0.f;
+  F3 ecur{0.f, 0.f, 0.f}, hcur{0.f, 0.f, 0.f};
+
+  // Faraday update of plane p into S.hc[p % 3] (all region cells); E of plane
+  // p is left in ecur, the curl-updated H in hcur.
+  auto curl = [&](int p, bool first) {
+    const float* R = raw0 + (p & (kRing - 1)) * kSlotF;
+    const float* R1 = raw0 + ((p + 1) & (kRing - 1)) * kSlotF;
+    const float ex = R[0];
+    const float ey = first ? R[kTileF] : cey;
+    const float ez = first ? R[2 * kTileF] : cez;
+    // row w + 1 of the last row and plane p + 1 of the last plane read
+    // in-bounds values that only feed results nobody uses
+    const float ex_j = R[kBoxK], ez_j = R[2 * kTileF + kBoxK];
+    const float ex_k = R[1], ey_k = R[kTileF + 1];
+    const float ey_i = R1[kTileF], ez_i = R1[2 * kTileF];
+    float vx = R[3 * kTileF], vy = R[4 * kTileF], vz = R[5 * kTileF];
     for (int q = 0; q < nh; ++q) {
       const wf_source& Q = P.src[S.L.h[q]];
       if (p >= Q.i0 && p < Q.i1 && gj >= Q.j0 && gj < Q.j1 && gk >= Q.k0 && gk < Q.k1) {
@@ -208,24 +226,30 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
         else vz = fadd(vz, v);
       }
     }
-    if (gj < ny - 1 && gk < nz - 1) {
+    const bool il = p < nx - 1;
+    if (cjk) {
       const float t1 = dv<FDIV>(fsub(ey_k, ey), dz, rdz);
       const float t2 = dv<FDIV>(fsub(ez_j, ez), dy, rdy);
       vx = fadd(vx, fmul(dh, fsub(t1, t2)));
     }
-    if (p < nx - 1 && gk < nz - 1) {
+    if (il && ck) {
       const float t1 = dv<FDIV>(fsub(ez_i, ez), dx, rdx);
       const float t2 = dv<FDIV>(fsub(ex_k, ex), dz, rdz);
       vy = fadd(vy, fmul(dh, fsub(t1, t2)));
     }
-    if (p < nx - 1 && gj < ny - 1) {
+    if (il && cj) {
       const float t1 = dv<FDIV>(fsub(ex_j, ex), dy, rdy);
       const float t2 = dv<FDIV>(fsub(ey_i, ey), dx, rdx);
       vz = fadd(vz, fmul(dh, fsub(t1, t2)));
     }
-    S.hc[h][0][w][lane] = vx;
-    S.hc[h][1][w][lane] = vy;
-    S.hc[h][2][w][lane] = vz;
+    float* H = hc0 + (p % 3) * kHcSetF;
+    H[0] = vx;
+    H[kHcF] = vy;
+    H[2 * kHcF] = vz;
+    ecur = F3{ex, ey, ez};
+    hcur = F3{vx, vy, vz};
+    cey = ey_i;
+    cez = ez_i;
   };
 
   // ---- prologue ---------------------------------------------------------------
@@ -235,7 +259,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   land(f0);
   if (f0 + 1 <= plast) land(f0 + 1);
   failed = __syncthreads_or(failed) != 0;
-  if (!failed) curl(f0);
+  if (!failed) curl(f0, true);
   F3 hprev{0.f, 0.f, 0.f};
   unsigned mxb[6] = {0u, 0u, 0u, 0u, 0u, 0u};
   const bool check = P.check_max != nullptr && P.n_check > 0 && (n + 1) % P.n_check == 0;
@@ -249,54 +273,70 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     failed = __syncthreads_or(failed) != 0;
     if (failed) break;
     if (tid == 0 && f + 3 <= plast) issue(f + 3);
-    if (p < nx) curl(p);
-    __syncthreads();  // B: hc(p) visible
-    // ---- Mur faces of plane f, as pure functions of old and curl-updated H ----
-    const int sf = f % kRing, sp = p % kRing, hf0 = f % 3, hp = p % 3, hm = (f + 2) % 3;
+    const F3 ef = ecur;  // E of plane f (sources included)
+    float hxF = hcur.x, hyF = hcur.y, hzF = hcur.z;
+    if (p < nx) curl(p, false);
+    const int sf = f & (kRing - 1), hf0 = f % 3;
     auto Ho = [&](int c, int ww, int ll) -> float { return S.raw[sf][3 + c][ww][ll + cofs]; };
-    auto Hc = [&](int c, int ww, int ll) -> float { return S.hc[hf0][c][ww][ll]; };
-    // Hy, Hz after the x faces
-    auto xf = [&](int c, int ww, int ll) -> float {
-      if (f == 0) return fadd(S.raw[sp][3 + c][ww][ll + cofs],
-                              fmul(mx, fsub(S.hc[hp][c][ww][ll], Ho(c, ww, ll))));
-      if (f == nx - 1) return fadd(S.hom[c - 1][ww][ll], fmul(mx, fsub(S.hc[hm][c][ww][ll], Ho(c, ww, ll))));
-      return Hc(c, ww, ll);
-    };
-    // Hx after the y faces (Hx has no x face)
-    auto yfx = [&](int ww, int ll) -> float {
-      const int g = j0 + ww;
-      if (g == 0 && ww + 1 < kTJ) return fadd(Ho(0, ww + 1, ll), fmul(my, fsub(Hc(0, ww + 1, ll), Ho(0, ww, ll))));
-      if (g == ny - 1 && ww >= 1) return fadd(Ho(0, ww - 1, ll), fmul(my, fsub(Hc(0, ww - 1, ll), Ho(0, ww, ll))));
-      return Hc(0, ww, ll);
-    };
-    float hxF = yfx(w, lane), hyF = xf(1, w, lane), hzF = xf(2, w, lane);
-    if (gj == 0 && w + 1 < kTJ)
-      hzF = fadd(Ho(2, w + 1, lane), fmul(my, fsub(xf(2, w + 1, lane), Ho(2, w, lane))));
-    else if (gj == ny - 1 && w >= 1)
-      hzF = fadd(Ho(2, w - 1, lane), fmul(my, fsub(xf(2, w - 1, lane), Ho(2, w, lane))));
-    if (zf_on && in) {
-      if (gk == 0 && lane + 1 < kTK) {
-        hxF = fadd(Ho(0, w, lane + 1), fmul(mz, fsub(yfx(w, lane + 1), Ho(0, w, lane))));
-        hyF = fadd(Ho(1, w, lane + 1), fmul(mz, fsub(xf(1, w, lane + 1), Ho(1, w, lane))));
-      } else if (gk == nz - 1 && lane >= 1) {
-        hxF = fadd(Ho(0, w, lane - 1), fmul(mz, fsub(yfx(w, lane - 1), Ho(0, w, lane))));
-        hyF = fadd(Ho(1, w, lane - 1), fmul(mz, fsub(xf(1, w, lane - 1), Ho(1, w, lane))));
-      }
-    }
-    S.hf[0][w][lane] = hxF;
-    S.hf[1][w][lane] = hyF;
-    S.hf[2][w][lane] = hzF;
     if (f == nx - 2) {
       S.hom[0][w][lane] = Ho(1, w, lane);
       S.hom[1][w][lane] = Ho(2, w, lane);
     }
-    __syncthreads();  // C: final H of plane f visible
+    const bool face = face_blk || f == 0 || f == nx - 1;  // uniform over the CTA
+    const float* Hn;  // final H of plane f, row-major [3][kTJ][kTK]
+    if (face) {
+      __syncthreads();  // B: hc(p) visible
+      // ---- Mur faces of plane f, as pure functions of old and curl-updated H ----
+      const int sp = p & (kRing - 1), hp = p % 3, hm = (f + 2) % 3;
+      auto Hc = [&](int c, int ww, int ll) -> float { return S.hc[hf0][c][ww][ll]; };
+      // Hy, Hz after the x faces
+      auto xf = [&](int c, int ww, int ll) -> float {
+        if (f == 0) return fadd(S.raw[sp][3 + c][ww][ll + cofs],
+                                fmul(mx, fsub(S.hc[hp][c][ww][ll], Ho(c, ww, ll))));
+        if (f == nx - 1) return fadd(S.hom[c - 1][ww][ll], fmul(mx, fsub(S.hc[hm][c][ww][ll], Ho(c, ww, ll))));
+        return Hc(c, ww, ll);
+      };
+      // Hx after the y faces (Hx has no x face)
+      auto yfx = [&](int ww, int ll) -> float {
+        const int g = j0 + ww;
+        if (g == 0 && ww + 1 < kTJ) return fadd(Ho(0, ww + 1, ll), fmul(my, fsub(Hc(0, ww + 1, ll), Ho(0, ww, ll))));
+        if (g == ny - 1 && ww >= 1) return fadd(Ho(0, ww - 1, ll), fmul(my, fsub(Hc(0, ww - 1, ll), Ho(0, ww, ll))));
+        return Hc(0, ww, ll);
+      };
+      hxF = yfx(w, lane);
+      hyF = xf(1, w, lane);
+      hzF = xf(2, w, lane);
+      if (gj == 0 && w + 1 < kTJ)
+        hzF = fadd(Ho(2, w + 1, lane), fmul(my, fsub(xf(2, w + 1, lane), Ho(2, w, lane))));
+      else if (gj == ny - 1 && w >= 1)
+        hzF = fadd(Ho(2, w - 1, lane), fmul(my, fsub(xf(2, w - 1, lane), Ho(2, w, lane))));
+      if (zf_on && in) {
+        if (gk == 0 && lane + 1 < kTK) {
+          hxF = fadd(Ho(0, w, lane + 1), fmul(mz, fsub(yfx(w, lane + 1), Ho(0, w, lane))));
+          hyF = fadd(Ho(1, w, lane + 1), fmul(mz, fsub(xf(1, w, lane + 1), Ho(1, w, lane))));
+        } else if (gk == nz - 1 && lane >= 1) {
+          hxF = fadd(Ho(0, w, lane - 1), fmul(mz, fsub(yfx(w, lane - 1), Ho(0, w, lane))));
+          hyF = fadd(Ho(1, w, lane - 1), fmul(mz, fsub(xf(1, w, lane - 1), Ho(1, w, lane))));
+        }
+      }
+      S.hf[0][w][lane] = hxF;
+      S.hf[1][w][lane] = hyF;
+      S.hf[2][w][lane] = hzF;
+      __syncthreads();  // C: final H of plane f visible
+      Hn = &S.hf[0][0][0];
+    } else {
+      // no face touches this block on this plane: the final H is the
+      // curl-updated H, already visible since barrier A
+      Hn = &S.hc[hf0][0][0][0];
+    }
     // ---- Ampere update and outputs of plane f ----
     if (f >= ia && core) {
-      const float hz_j = S.hf[2][w - 1][lane], hx_j = S.hf[0][w - 1][lane];
-      const float hy_k = S.hf[1][w][lane - 1], hx_k = S.hf[0][w][lane - 1];
-      float ex = S.raw[sf][0][w][col], ey = S.raw[sf][1][w][col], ez = S.raw[sf][2][w][col];
-      const float cav = MAT ? S.raw[sf][6][w][col] : 0.f, cbv = MAT ? S.raw[sf][7][w][col] : 0.f;
+      const float* N = Hn + (w * kTK + lane);
+      const float hz_j = N[2 * kHcF - kTK], hx_j = N[-kTK];
+      const float hy_k = N[kHcF - 1], hx_k = N[-1];
+      float ex = ef.x, ey = ef.y, ez = ef.z;
+      const float* R = raw0 + sf * kSlotF;
+      const float cav = MAT ? R[6 * kTileF] : 0.f, cbv = MAT ? R[7 * kTileF] : 0.f;
       if (gj >= 1 && gk >= 1) {
         const float c = fsub(dv<FDIV>(fsub(hzF, hz_j), dy, rdy), dv<FDIV>(fsub(hyF, hy_k), dz, rdz));
         ex = MAT ? fadd(fmul(cav, ex), fmul(cbv, c)) : fadd(ex, fmul(de, c));
