@@ -8,7 +8,10 @@
 // changes is data movement: one thread issues, per i-plane, one
 // cp.async.bulk.tensor load per array (Ex, Ey, Ez, Hx, Hy, Hz and Ca, Cb) of a
 // 16 x 36 box into a 4-slot shared-memory ring, completing on the slot's
-// mbarrier; plane f+3 is in flight while plane f is finished.  All
+// mbarrier.  A thread keeps E, Ca and Cb of its cell of plane f in registers
+// from the Faraday step of that plane, so plane f's slot is refilled with
+// plane f + 4 as soon as the plane-f step starts (after the Mur code on face
+// planes): planes f + 3 and f + 4 are in flight while plane f is finished.  All
 // neighbours (j +- 1, k +- 1, i +- 1) are read from shared memory, so no
 // thread issues global loads, shuffles or address arithmetic for them.  The
 // box starts at k = floor4(k0 - 1) (a TMA box must start on a 16-byte
@@ -94,7 +97,6 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   const int inst = blockIdx.y;
   if (inst) {
     const long long q = inst;
-    for (int c = 0; c < 6; ++c) P.out[c] += q * P.fstride;
     P.traces += q * P.tstride;
     P.src += q * P.sstride;
   }
@@ -112,7 +114,8 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   const int f0 = max(ia - 1, 0);
   const int plast = min(nx - 1, ib + 1);  // last plane the segment reads
   const long long PS = (long long)ny * nz;
-  const long long colg = in ? (long long)gj * nz + gk : 0;
+  // output offset of this column, instance included (P.out stays unmodified)
+  const long long colg = (in ? (long long)gj * nz + gk : 0) + (long long)inst * P.fstride;
   const float dh = P.dh, de = P.de, dx = P.dx, dy = P.dy, dz = P.dz;
   const float mx = P.mx, my = P.my, mz = P.mz;
   const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy),
@@ -199,12 +202,12 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   // on the planes i = 0 and i = Nx - 1
   const bool face_blk = !(j0 >= 1 && j0 + kTJ - 1 <= ny - 2 && k0 >= 1 && k0 + kTK - 1 <= nz - 2);
   // carried between planes: Ey, Ez of plane p (read as the i + 1 neighbours
-  // of plane p - 1), E of the plane being finished, curl-updated H
-  float cey = 0.f, cez = 0.f;
+  // of plane p - 1), E, Ca, Cb of the plane being finished, curl-updated H
+  float cey = 0.f, cez = 0.f, cca = 0.f, ccb = 0.f;
   F3 ecur{0.f, 0.f, 0.f}, hcur{0.f, 0.f, 0.f};
 
-  // Faraday update of plane p into S.hc[p % 3] (all region cells); E of plane
-  // p is left in ecur, the curl-updated H in hcur.
+  // Faraday update of plane p into S.hc[p % 3] (all region cells); E, Ca, Cb
+  // of plane p are left in ecur, cca, ccb, the curl-updated H in hcur.
   auto curl = [&](int p, bool first) {
     const float* R = raw0 + (p & (kRing - 1)) * kSlotF;
     const float* R1 = raw0 + ((p + 1) & (kRing - 1)) * kSlotF;
@@ -248,13 +251,17 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     H[2 * kHcF] = vz;
     ecur = F3{ex, ey, ez};
     hcur = F3{vx, vy, vz};
+    if (MAT) {
+      cca = R[6 * kTileF];
+      ccb = R[7 * kTileF];
+    }
     cey = ey_i;
     cez = ez_i;
   };
 
   // ---- prologue ---------------------------------------------------------------
   if (tid == 0) {
-    for (int p = f0; p <= min(f0 + 2, plast); ++p) issue(p);
+    for (int p = f0; p <= min(f0 + kRing - 1, plast); ++p) issue(p);
   }
   land(f0);
   if (f0 + 1 <= plast) land(f0 + 1);
@@ -268,12 +275,18 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   for (int f = f0; f < ib && !failed; ++f) {
     const int p = f + 1;
     if (f + 2 <= plast) land(f + 2);
-    // A: slot of plane f-1 is free; injections and hc(f) visible; a timed-out
-    // wait anywhere stops the whole CTA
+    // A: injections and hc(f) visible; a timed-out wait anywhere stops the
+    // whole CTA
     failed = __syncthreads_or(failed) != 0;
     if (failed) break;
-    if (tid == 0 && f + 3 <= plast) issue(f + 3);
+    const bool face = face_blk || f == 0 || f == nx - 1;  // uniform over the CTA
+    // plane f's slot takes plane f + 4 once nothing reads it: right after
+    // barrier A (Ca, Cb and E of plane f are in registers; the old H of plane
+    // Nx - 2 is read below, but no plane is issued then) unless the Mur code
+    // reads plane f's old H, then after barrier C
+    if (!face && tid == 0 && f + kRing <= plast) issue(f + kRing);
     const F3 ef = ecur;  // E of plane f (sources included)
+    const float cav = cca, cbv = ccb;
     float hxF = hcur.x, hyF = hcur.y, hzF = hcur.z;
     if (p < nx) curl(p, false);
     const int sf = f & (kRing - 1), hf0 = f % 3;
@@ -282,7 +295,6 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       S.hom[0][w][lane] = Ho(1, w, lane);
       S.hom[1][w][lane] = Ho(2, w, lane);
     }
-    const bool face = face_blk || f == 0 || f == nx - 1;  // uniform over the CTA
     const float* Hn;  // final H of plane f, row-major [3][kTJ][kTK]
     if (face) {
       __syncthreads();  // B: hc(p) visible
@@ -322,7 +334,8 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       S.hf[0][w][lane] = hxF;
       S.hf[1][w][lane] = hyF;
       S.hf[2][w][lane] = hzF;
-      __syncthreads();  // C: final H of plane f visible
+      __syncthreads();  // C: final H of plane f visible; plane f's slot unread
+      if (tid == 0 && f + kRing <= plast) issue(f + kRing);
       Hn = &S.hf[0][0][0];
     } else {
       // no face touches this block on this plane: the final H is the
@@ -335,8 +348,6 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       const float hz_j = N[2 * kHcF - kTK], hx_j = N[-kTK];
       const float hy_k = N[kHcF - 1], hx_k = N[-1];
       float ex = ef.x, ey = ef.y, ez = ef.z;
-      const float* R = raw0 + sf * kSlotF;
-      const float cav = MAT ? R[6 * kTileF] : 0.f, cbv = MAT ? R[7 * kTileF] : 0.f;
       if (gj >= 1 && gk >= 1) {
         const float c = fsub(dv<FDIV>(fsub(hzF, hz_j), dy, rdy), dv<FDIV>(fsub(hyF, hy_k), dz, rdz));
         ex = MAT ? fadd(fmul(cav, ex), fmul(cbv, c)) : fadd(ex, fmul(de, c));
