@@ -634,17 +634,114 @@ def bench_adjoint(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def bench_dataset(args, ws, rank, local):
+    """Brain dataset generation at the reference generator's defaults (64^3,
+    3 mm, 8-element ring r = 30 cells, 300 steps, 1 GHz): one step = one
+    sample (two phantoms painted, both MIMO acquisitions as one batched
+    2 x 8-member solve, scattered signals, DAS image, compressed .npz)."""
+    import tempfile
+    import oracle
+    from waveforge_b200.datasets import BrainDatasetGenerator
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n, n_tx, steps = args.side or 64, 8, args.nsteps
+    tmp = tempfile.TemporaryDirectory()
+    gen = BrainDatasetGenerator(tmp.name, grid_size=n, dx_mm=3.0, n_tx=n_tx,
+                                ring_radius_cells=min(30, n // 2 - 2), n_steps=steps,
+                                device=str(dev), seed=args.seed, verbose=False)
+    counter = iter(range(10 ** 9))
+
+    def one():
+        i = next(counter)
+        smp = gen.generate_sample(label=i % 4, seed=args.seed * 1000 + i)
+        if smp is not None:
+            gen.save_sample(smp, i)
+        return smp
+
+    def plain():
+        """The same two acquisitions, one solve at a time (the reference's
+        per-transmitter loop on this library's kernels)."""
+        from waveforge_b200.datasets.brain import BrainPhantom3D, sample_random_geometry
+        ph = BrainPhantom3D(gen.grid, 1e9, geometry=sample_random_geometry(args.seed, n, 3.0),
+                            seed=args.seed)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            for t in range(n_tx):
+                gen._run_simulation(ph, t)
+        torch.cuda.synchronize(dev)
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize(dev)
+    barrier(ws)
+    clk = ClockSampler(local)
+    clk.start()
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        done += one() is not None
+    torch.cuda.synchronize(dev)
+    el = time.perf_counter() - t0
+    clocks = clk.stop()
+    el = reduce_max(el, ws, dev)
+    plain_s = plain() if rank == 0 and not args.no_plain else None
+    upd = 2 * n_tx * n ** 3 * steps
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            from waveforge_b200.datasets.brain import BrainPhantom3D, sample_random_geometry
+            from waveforge_b200.core.grid import YeeGrid
+            gh = YeeGrid(n, n, 3e-3, 3e-3, Nz=n, dz=3e-3, device="cpu")
+            ph = BrainPhantom3D(gh, 1e9, geometry=sample_random_geometry(args.seed, n, 3.0),
+                                seed=args.seed)
+            ca, cb = ph.build()
+            pos = gen.ring.positions
+            wave = gen._waveform().build(steps, gh.dt, "cpu")
+
+            def make_oracle():
+                o = oracle.Oracle3D(n, n, n, gh.dx, gh.dy, gh.dz, gh.dt, ca, cb)
+                o.add_point_source("Ez", pos[0][0], pos[0][1], wave, k=pos[0][2])
+                return o, [("Ez", i, j, k) for i, j, k in pos]
+            v, cores, sample = cpu_single_sample(make_oracle, n ** 3, steps, args.ref_budget)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": "one transmitter solve of a sample: " + sample}
+        rate = ws * done / el
+        h2d = 2 * 2 * n ** 3 * 4
+        d2h = 2 * n_tx * n_tx * steps * 4
+        line = {
+            "metric": "dataset samples/s (brain haemorrhage, 2 x 8-TX MIMO per sample)",
+            "value": rate, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"brain_dataset_{n}^3_3mm_{n_tx}tx_{steps}steps",
+                       "cell_updates_per_sample": upd, "parallelism": f"replicas x{ws}",
+                       "note": "wall clock per sample: host phantom paint, one batched solve of "
+                               "all 16 acquisitions, DAS, npz write"},
+            "gcell_upd_per_s": rate * upd / 1e9,
+            "plain_per_solve_samples_per_s": None if plain_s is None else 1.0 / plain_s,
+            "e2e": {"value": rate, "unit": "samples/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "cpu_baseline": cpu, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    tmp.cleanup()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mimo", choices=["mimo", "plain2d", "head3d", "serve", "adjoint"],
+    ap.add_argument("--workload", default="mimo",
+                    choices=["mimo", "plain2d", "head3d", "serve", "adjoint", "dataset"],
                     help="mimo: batched uneven breast MIMO (default, the headline metric); "
                          "plain2d: one 4096^2 lossy 2D solve; head3d: one 256^3 head solve; "
                          "serve: Poisson request stream through the continuous-batching server; "
-                         "adjoint: one misfit gradient (forward + adjoint) of a 512^2 16-TX phantom")
+                         "adjoint: one misfit gradient (forward + adjoint) of a 512^2 16-TX phantom; "
+                         "dataset: brain dataset samples (two batched 8-TX MIMO acquisitions each)")
     ap.add_argument("--batch-mode", default="auto", choices=["persistent", "tiled", "auto"],
                     help="mimo: one persistent launch per batch, one tile-queue launch per pass, "
                          "or the autotuner's pick (default)")
@@ -676,7 +773,7 @@ def main():
         raise SystemExit("--warmup must be >= 3")
     if args.nsteps is None:
         args.nsteps = {"mimo": 3000, "plain2d": 2000, "head3d": 1500, "serve": 0,
-                       "adjoint": 1000}[args.workload]
+                       "adjoint": 1000, "dataset": 300}[args.workload]
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
@@ -684,6 +781,10 @@ def main():
         return
     if args.workload == "adjoint":
         bench_adjoint(args, ws, rank, local)
+        barrier(ws)
+        return
+    if args.workload == "dataset":
+        bench_dataset(args, ws, rank, local)
         barrier(ws)
         return
     if args.workload == "serve":

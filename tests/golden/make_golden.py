@@ -446,6 +446,65 @@ def case_antenna(R, ref: Path, out):
                         **res)
 
 
+def case_brain_dataset(R, ref: Path, out):
+    """The brain dataset path (src/datasets): Cole-Cole tissue values, seeded
+    head geometries, seeded bleed placement, a phantom's Ca/Cb digests, and
+    whole generator samples (both MIMO acquisitions, scattered signals, DAS
+    image, metadata, saved .npz key set) at 40^3 / 6 mm / 4 antennas."""
+    import tempfile
+    from datasets.brain import tissue_library as TL
+    from datasets.brain.phantom import BrainPhantom3D, sample_random_geometry
+    from datasets.generator import BrainDatasetGenerator
+    res = {}
+    names = sorted(TL.TISSUES) + [f"blood_{a}" for a in ("acute", "subacute", "chronic")]
+    res["tissue_names"] = np.array(names)
+    for f in (0.5e9, 1e9, 2e9, 6.5e9):
+        t = TL.all_tissues_at_freq(f)
+        res[f"tissue_{int(f)}"] = np.array([t[n] for n in names], dtype=np.float64)
+    geoms = []
+    for grid_size, dx_mm in ((64, 3.0), (48, 4.0), (40, 6.0)):
+        for seed in range(12):
+            g = sample_random_geometry(seed * 37 + 5, grid_size, dx_mm)
+            geoms.append([grid_size, int(dx_mm * 10), seed * 37 + 5, *g.center, g.scalp_outer_r,
+                          g.skull_outer_r, g.skull_inner_r, g.dura_inner_r, g.csf_inner_r,
+                          g.gray_matter_r, g.white_matter_r])
+    res["geoms"] = np.array(geoms, dtype=np.int64)
+    grid64 = R["grid"].YeeGrid(64, 64, dx=3e-3, dy=3e-3, Nz=64, dz=3e-3, device="cpu")
+    bleeds = []
+    for q, (btype, age, size) in enumerate([(b, a, z) for b in ("epidural", "subdural", "intracerebral")
+                                            for a in ("acute", "chronic") for z in ("small", "large")]):
+        geom = sample_random_geometry(100 + q, 64, 3.0)
+        ph = BrainPhantom3D(grid64, 1e9, geometry=geom, seed=200 + q)
+        b = ph.add_random_bleed(btype, age, size)
+        bleeds.append([100 + q, 200 + q] + ([-1, -1, -1, -1, 0, 0] if b is None else
+                                            [*b.center, b.radius, b.eps_r, b.sigma]))
+    res["bleeds"] = np.array(bleeds, dtype=np.float64)
+    res["bleed_cases"] = np.array([f"{b}/{a}/{z}" for b in ("epidural", "subdural", "intracerebral")
+                                   for a in ("acute", "chronic") for z in ("small", "large")])
+    geom = sample_random_geometry(7, 64, 3.0)
+    ph = BrainPhantom3D(grid64, 1e9, geometry=geom, seed=9)
+    ph.add_bleed_at((40, 30, 28), 4, "intracerebral", "subacute")
+    ca, cb = ph.build()
+    res["phantom64_ca_sha"], res["phantom64_cb_sha"] = sha(ca), sha(cb)
+    with tempfile.TemporaryDirectory() as tmp:
+        for tag, kw, label, seed in (("nb", {}, 3, 11), ("nb0", {}, 0, 4),
+                                     ("uwb", {"freq_low_hz": 1e9, "freq_high_hz": 3e9}, 1, 23)):
+            gen = BrainDatasetGenerator(tmp, grid_size=40, dx_mm=6.0, n_tx=4, ring_radius_cells=18,
+                                        n_steps=700, device="cpu", seed=0, **kw)
+            smp = gen.generate_sample(label=label, seed=seed)
+            path = gen.save_sample(smp, 0)
+            res[f"{tag}_label"], res[f"{tag}_seed"] = label, seed
+            for k in ("signals_total", "signals_reference", "signals_scattered", "das_image",
+                      "bleed_center_cells", "bleed_radius_cells", "phantom_skull_inner_r",
+                      "phantom_gray_r", "phantom_scalp_outer_r", "dt_s", "freq_hz"):
+                res[f"{tag}_{k}"] = np.asarray(smp[k])
+            res[f"{tag}_bleed"] = np.array([smp["bleed_type"], smp["bleed_age"]])
+            res[f"{tag}_sha_total"] = sha(smp["signals_total"])
+            res[f"{tag}_sha_reference"] = sha(smp["signals_reference"])
+            res[f"{tag}_npz_keys"] = np.array(sorted(np.load(path, allow_pickle=True).files))
+    np.savez_compressed(out / "brain_dataset40.npz", **res)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -464,6 +523,7 @@ def main():
         "edges3d": lambda: case_edges_3d(R, out),
         "das": lambda: case_das(R, ref, out),
         "antenna": lambda: case_antenna(R, ref, out),
+        "brain": lambda: case_brain_dataset(R, ref, out),
     }
     for k, fn in todo.items():
         if a.only and k not in a.only.split(","):

@@ -16,7 +16,8 @@ from typing import Optional
 import torch
 
 from .. import _native as nat
-from ._engine import EngineBase, ProbeTable, SimulationDivergedError, tune_struct  # noqa: F401
+from ._engine import (EngineBase, ProbeTable, SimulationDivergedError, SourceTable,  # noqa: F401
+                      source_list, tune_struct)
 from .fields import FIELD_COMPONENTS, FieldSet
 from .grid import YeeGrid
 
@@ -32,7 +33,12 @@ class FDTD3D(EngineBase):
 
     def __init__(self, grid: YeeGrid, fields: FieldSet, boundary: object, sources: Optional[object] = None,
                  *, Ca: Optional[torch.Tensor] = None, Cb: Optional[torch.Tensor] = None,
-                 stability_threshold: float = 1e10, n_check: int = 100, tune=None) -> None:
+                 stability_threshold: float = 1e10, n_check: int = 100, tune=None,
+                 member_sources: Optional[list] = None) -> None:
+        """``member_sources`` (new; batched FieldSet only): one source object
+        per batch member -- e.g. one transmitter per member -- instead of the
+        reference's broadcast of ``sources`` to every member.  Every member
+        must inject the same number of source boxes."""
         if grid.Nx < 4:
             raise ValueError(f"grid.Nx must be >= 4 for a valid 3D Yee stencil, got {grid.Nx}")
         if grid.Ny < 4:
@@ -72,6 +78,16 @@ class FDTD3D(EngineBase):
                                nat.fastdiv_flags(self._device, dx, dy, dz))
         self._tune = tune_struct(tune)
         self._scratch: Optional[torch.Tensor] = None
+        self._member_sources = None
+        self._member_table = None
+        if member_sources is not None:
+            if not fields.is_batched or len(member_sources) != fields.batch_size:
+                raise ValueError("member_sources needs a batched FieldSet and one entry per member")
+            if sources is not None:
+                raise ValueError("give either sources (broadcast) or member_sources, not both")
+            if tune is not None or grid.Nz == 1:
+                raise ValueError("member_sources runs on the default 3D streaming kernel")
+            self._member_sources = list(member_sources)
 
     def compile_step(self, *, backend: str = "inductor", mode: str = "reduce-overhead") -> None:
         """Kept for API compatibility: the step is already one fused CUDA launch."""
@@ -93,7 +109,8 @@ class FDTD3D(EngineBase):
                  traces: Optional[torch.Tensor] = None) -> None:
         if nsteps <= 0:
             return
-        src = self._sources_table(FIELD_COMPONENTS, 3)
+        src = self._sources_table(FIELD_COMPONENTS, 3) if self._member_sources is None \
+            else self._members_table()
         step0 = self.steps_completed
         src.check_range(step0, nsteps)
         g = self._grid
@@ -129,6 +146,17 @@ class FDTD3D(EngineBase):
         self.steps_completed += nsteps
         self._process_checks(chk, count, step0)
 
+    def _members_table(self) -> SourceTable:
+        """One table of every member's source boxes, member after member."""
+        if self._member_table is None:
+            per = [sum(len(s.native_boxes()) for s in source_list(m)) for m in self._member_sources]
+            if len(set(per)) != 1:
+                raise ValueError(f"member_sources inject different numbers of boxes: {per}")
+            inj = [s for m in self._member_sources for s in source_list(m)]
+            self._member_table = SourceTable(inj, self._device, FIELD_COMPONENTS, 3)
+            self._member_per = per[0]
+        return self._member_table
+
     def _advance_batched(self, nsteps, src, probes, traces, chk, step0) -> None:
         """All batch members in one launch per step (wf_fdtd3d_batch_run):
         every member gets the same sources, as the reference broadcasts them
@@ -153,9 +181,12 @@ class FDTD3D(EngineBase):
                 raise ValueError("Ca / Cb must be (Nx, Ny, Nz) or (B, Nx, Ny, Nz)")
         fp = (ctypes.c_void_p * 6)(*[t.data_ptr() for t in comps])
         sp = (ctypes.c_void_p * 6)(*[self._scratch[c].data_ptr() for c in range(6)])
+        per, sstride = src.count, 0
+        if self._member_sources is not None:
+            per = sstride = self._member_per
         nat.check(nat.load().wf_fdtd3d_batch_run(
             ctypes.byref(self._g), B, n, fp, sp, nat.ptr(ca), nat.ptr(cb), cstride, src.ptr,
-            src.count, 0, None if probes is None else probes.ptr,
+            per, sstride, None if probes is None else probes.ptr,
             0 if probes is None else probes.count, None if traces is None else traces.data_ptr(),
             0 if traces is None else traces.stride(-2),
             0 if traces is None else traces.stride(0), step0, step0, nsteps,
