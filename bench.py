@@ -707,7 +707,9 @@ def bench_dataset(args, ws, rank, local):
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                    "sample": "one transmitter solve of a sample: " + sample}
         rate = ws * done / el
-        h2d = 2 * 2 * n ** 3 * 4
+        # per sample: two phantoms' region lists (<= 7 spheres x 40 B) and
+        # material tables (<= 8 x 8 B) cross to the device; Ca/Cb are painted there
+        h2d = 2 * (7 * 40 + 8 * 8)
         d2h = 2 * n_tx * n_tx * steps * 4
         line = {
             "metric": "dataset samples/s (brain haemorrhage, 2 x 8-TX MIMO per sample)",
@@ -717,8 +719,9 @@ def bench_dataset(args, ws, rank, local):
             "data": "synthetic",
             "config": {"workload": f"brain_dataset_{n}^3_3mm_{n_tx}tx_{steps}steps",
                        "cell_updates_per_sample": upd, "parallelism": f"replicas x{ws}",
-                       "note": "wall clock per sample: host phantom paint, one batched solve of "
-                               "all 16 acquisitions, DAS, npz write"},
+                       "note": "wall clock per sample: seeded geometry and bleed placement on "
+                               "the host, both phantoms painted on the device, one batched solve "
+                               "of all 16 acquisitions, DAS, compressed npz write"},
             "gcell_upd_per_s": rate * upd / 1e9,
             "plain_per_solve_samples_per_s": None if plain_s is None else 1.0 / plain_s,
             "e2e": {"value": rate, "unit": "samples/s", "h2d_bytes_per_step": h2d,

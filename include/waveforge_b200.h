@@ -332,6 +332,35 @@ int32_t wf_paint2d(int32_t nx, int32_t ny, const wf_region2d* regions, int32_t n
                    float* ca, float* cb, double* eps_r, double* sigma,
                    int32_t* status, void* stream);
 
+/* One region of a painted 3D material map (painter's order: later regions
+ * win), parameters float32-rounded as in wf_region2d
+ * (MaterialMap3D, src/core/materials.py:297-423):
+ *  WF_REGION3_SPHERE     p = ci, cj, ck, r*r                  (add_sphere)
+ *  WF_REGION3_BOX        p = i0, i1, j0, j1, k0, k1           (add_box)
+ *  WF_REGION3_ELLIPSOID  p = ci, cj, ck, a*a, b*b, c*c        (add_ellipsoid)
+ *  WF_REGION3_CYL_X/Y/Z  p = ci, cj, ck, r*r, height/2        (add_cylinder) */
+#define WF_REGION3_SPHERE    0
+#define WF_REGION3_BOX       1
+#define WF_REGION3_ELLIPSOID 2
+#define WF_REGION3_CYL_X     3
+#define WF_REGION3_CYL_Y     4
+#define WF_REGION3_CYL_Z     5
+typedef struct wf_region3d {
+  int32_t kind;
+  int32_t material;
+  float p[8];
+} wf_region3d;
+
+/* Paint Ca/Cb (nx*ny*nz float32 each, [i][j][k]) on the device,
+ * bit-identical to MaterialMap3D.build3d (src/core/materials.py:425-478)
+ * for the same regions.  regions: device array; table_ca/cb: nmat float32 on
+ * the device (index 0 = default material).  A region whose material index is
+ * outside [0, nmat) paints the default and sets *status (device, nullable)
+ * to WF_E_ARG.  At most 1024 regions. */
+int32_t wf_paint3d(int32_t nx, int32_t ny, int32_t nz, const wf_region3d* regions, int32_t nreg,
+                   const float* table_ca, const float* table_cb, int32_t nmat, float* ca,
+                   float* cb, int32_t* status, void* stream);
+
 /* Delay-and-sum backprojection on the device, bit-identical to the reference
  * NumPy float64 path of examples/brain_mimo_imaging.py:211-266 (and its
  * variants through px/py, gate_start, skip_self).

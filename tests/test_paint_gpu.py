@@ -73,3 +73,60 @@ def test_device_painter_rejects_custom_masks(cuda):
     mm = MaterialMap(g).add_custom(lambda I, J: I > J, Material("tri", 3.0, 0.0))
     with pytest.raises(ValueError):
         mm.build_device(cuda)
+
+
+# ---- 3D painter (wf_paint3d) against MaterialMap3D.build3d -------------------
+
+def _both3d(mm, cuda):
+    ca, cb = mm.build3d()
+    cad, cbd = mm.build3d_device(cuda)
+    return (ca, cb), (cad.cpu(), cbd.cpu())
+
+
+def test_device_painter_3d_random_primitives(cuda):
+    """Spheres, boxes, ellipsoids and cylinders on all three axes, with
+    centres on and between cells, overlapping in painter's order."""
+    from waveforge_b200.core.materials import MaterialMap3D
+    rng = np.random.default_rng(8)
+    g = YeeGrid(37, 29, 1e-3, 1e-3, Nz=44, dz=1e-3, courant=0.5, device="cpu")
+    mm = MaterialMap3D(g, default=Material("bg", 2.0, 0.01))
+    for q in range(40):
+        m = Material(f"m{q}", float(rng.uniform(1, 60)), float(rng.uniform(0, 1.5)))
+        c = tuple(float(v) for v in rng.uniform(-3, 45, 3).round(1 if q % 2 else 0))
+        kind = q % 6
+        if kind == 0:
+            mm.add_sphere(c, float(rng.uniform(1, 12)), m)
+        elif kind == 1:
+            lo = rng.uniform(-2, 30, 3).round(1)
+            mm.add_box(tuple(lo), tuple(lo + rng.uniform(1, 15, 3).round(1)), m)
+        elif kind == 2:
+            mm.add_ellipsoid(c, tuple(rng.uniform(1.5, 14, 3)), m)
+        else:
+            mm.add_cylinder(c, "xyz"[kind - 3], float(rng.uniform(1, 9)),
+                            float(rng.uniform(2, 30)), m)
+    (ca, cb), (cad, cbd) = _both3d(mm, cuda)
+    assert torch.equal(ca, cad) and torch.equal(cb, cbd)
+
+
+def test_device_painter_3d_brain_phantom_golden(cuda):
+    """The head phantom painted on the device gives the reference's Ca/Cb
+    digests (golden brain_dataset40.npz)."""
+    import hashlib
+    from conftest import GOLDEN
+    from waveforge_b200.datasets.brain import BrainPhantom3D, sample_random_geometry
+    d = np.load(GOLDEN / "brain_dataset40.npz")
+    g = YeeGrid(64, 64, 3e-3, 3e-3, Nz=64, dz=3e-3, device=cuda)
+    ph = BrainPhantom3D(g, 1e9, geometry=sample_random_geometry(7, 64, 3.0), seed=9)
+    ph.add_bleed_at((40, 30, 28), 4, "intracerebral", "subacute")
+    ca, cb = ph.build_device(cuda)
+    h = lambda t: hashlib.sha256(t.cpu().contiguous().numpy().tobytes()).hexdigest()
+    assert h(ca) == str(d["phantom64_ca_sha"]) and h(cb) == str(d["phantom64_cb_sha"])
+
+
+def test_device_painter_3d_rejects_custom_masks(cuda):
+    from waveforge_b200.core.materials import MaterialMap3D
+    g = YeeGrid(8, 8, 1e-3, 1e-3, Nz=8, dz=1e-3, device="cpu")
+    mm = MaterialMap3D(g).add_custom3d(lambda I, J, K: I > 3, Material("x", 3.0, 0.0))
+    assert not mm.device_paintable3d
+    with pytest.raises(ValueError):
+        mm.build3d_device(cuda)

@@ -264,12 +264,15 @@ class MaterialMap3D(MaterialMap):
         super().__init__(grid, default)
         self._regions3d: list = []
         self._materials3d: list[Material] = []
+        # typed description of each 3D region for the device painter (None = custom mask)
+        self._prims3d: list = []
 
     def add_sphere(self, center: tuple, radius: float, material: Material) -> "MaterialMap3D":
         ci, cj, ck = (float(c) for c in center)
         r2 = radius * radius
         self._regions3d.append(lambda I, J, K: (I - ci) ** 2 + (J - cj) ** 2 + (K - ck) ** 2 <= r2)
         self._materials3d.append(material)
+        self._prims3d.append((0, (ci, cj, ck, r2)))
         return self
 
     def add_cylinder(self, center: tuple, axis: str, radius: float, height: float,
@@ -284,6 +287,7 @@ class MaterialMap3D(MaterialMap):
             fn = lambda I, J, K: ((I - ci) ** 2 + (J - cj) ** 2 <= r2) & ((K - ck).abs() <= h2)
         self._regions3d.append(fn)
         self._materials3d.append(material)
+        self._prims3d.append(({"x": 3, "y": 4}.get(axis, 5), (ci, cj, ck, r2, h2)))
         return self
 
     def add_box(self, corner_min: tuple, corner_max: tuple, material: Material) -> "MaterialMap3D":
@@ -292,6 +296,7 @@ class MaterialMap3D(MaterialMap):
         self._regions3d.append(lambda I, J, K: (I >= i0) & (I <= i1) & (J >= j0) & (J <= j1)
                                & (K >= k0) & (K <= k1))
         self._materials3d.append(material)
+        self._prims3d.append((1, (i0, i1, j0, j1, k0, k1)))
         return self
 
     def add_ellipsoid(self, center: tuple, semi_axes: tuple, material: Material) -> "MaterialMap3D":
@@ -300,12 +305,65 @@ class MaterialMap3D(MaterialMap):
         self._regions3d.append(
             lambda I, J, K: (I - ci) ** 2 / a2 + (J - cj) ** 2 / b2 + (K - ck) ** 2 / c2 <= 1.0)
         self._materials3d.append(material)
+        self._prims3d.append((2, (ci, cj, ck, a2, b2, c2)))
         return self
 
     def add_custom3d(self, mask_fn, material: Material) -> "MaterialMap3D":
         self._regions3d.append(mask_fn)
         self._materials3d.append(material)
+        self._prims3d.append(None)
         return self
+
+    @property
+    def device_paintable3d(self) -> bool:
+        """True when every 3D region is a sphere, box, ellipsoid or cylinder."""
+        return all(p is not None for p in self._prims3d)
+
+    def build3d_device(self, device=None, out: tuple | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+        """``(Ca, Cb)``, each ``(Nx, Ny, Nz)`` float32 painted on ``device``
+        (default ``grid.device``) by ``wf_paint3d``, bit-identical to
+        ``build3d()``.  Only the region list and the material table cross to
+        the device.  ``out``: optional (Ca, Cb) tensors to fill.  The
+        Ca <= 0 check runs on the material table (no device sync)."""
+        from .. import _native as nat
+        if not self.device_paintable3d:
+            raise ValueError("build3d_device needs sphere/box/ellipsoid/cylinder regions only "
+                             "(add_custom3d masks are host-only: use build3d())")
+        dev = torch.device(device if device is not None else self._grid.device)
+        if dev.type != "cuda":
+            raise RuntimeError("build3d_device paints on a CUDA device only (use build3d())")
+        g = self._grid
+        dt = g.dt
+        mats = [self._default, *self._materials3d]
+        tca = torch.tensor([m.ca(dt) for m in mats], dtype=torch.float32)
+        tcb = torch.tensor([m.cb(dt) for m in mats], dtype=torch.float32)
+        _check_ca(tca, three_d=True)
+        regs = (nat.WfRegion3D * max(1, len(self._prims3d)))()
+        for q, (kind, params) in enumerate(self._prims3d):
+            regs[q].kind = kind
+            regs[q].material = q + 1
+            for t, v in enumerate(params):
+                regs[q].p[t] = nat.f32(v)
+        rb = bytes(memoryview(regs).cast("B"))
+        host = torch.cat([torch.frombuffer(bytearray(rb), dtype=torch.uint8),
+                          tca.view(torch.uint8), tcb.view(torch.uint8)]).pin_memory()
+        blob = host.to(dev, non_blocking=True)
+        base, nm = blob.data_ptr(), len(mats)
+        shape = (g.Nx, g.Ny, g.Nz)
+        if out is None:
+            ca = torch.empty(shape, dtype=torch.float32, device=dev)
+            cb = torch.empty(shape, dtype=torch.float32, device=dev)
+        else:
+            ca, cb = out
+            for t in (ca, cb):
+                if t.dtype != torch.float32 or not t.is_contiguous() or t.numel() != g.Nx * g.Ny * g.Nz:
+                    raise ValueError("out tensors must be contiguous float32 with Nx*Ny*Nz cells")
+        nat.check(nat.load().wf_paint3d(g.Nx, g.Ny, g.Nz, base, len(self._prims3d),
+                                        base + len(rb), base + len(rb) + 4 * nm, nm,
+                                        ca.data_ptr(), cb.data_ptr(), None,
+                                        nat.stream_handle(dev)))
+        self._keep = (host, blob)
+        return ca, cb
 
     def _paint3d(self):
         nx, ny, nz = self._grid.Nx, self._grid.Ny, self._grid.Nz

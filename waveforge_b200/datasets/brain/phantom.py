@@ -5,7 +5,8 @@ Concentric spheres, outside in: scalp, skull, dura, CSF, gray matter, white
 matter, painted in that order, then any bleeds on top.  Geometry and bleed
 placement are drawn from ``random.Random(seed)`` with the same sequence of
 draws as the reference (phantom.py:86-179 and :285-372), so a seed gives the
-same phantom -- and, through ``MaterialMap3D.build3d``, bit-identical Ca/Cb.
+same phantom -- and, through ``MaterialMap3D.build3d``, bit-identical Ca/Cb;
+``build_device`` paints the same coefficients on the GPU.
 """
 
 from __future__ import annotations
@@ -211,6 +212,12 @@ class BrainPhantom3D:
     def build(self) -> tuple[torch.Tensor, torch.Tensor]:
         """(Ca, Cb), each (Nx, Ny, Nz) float32 on the grid's device."""
         return self.material_map().build3d()
+
+    def build_device(self, device=None) -> tuple[torch.Tensor, torch.Tensor]:
+        """The same (Ca, Cb) painted on a CUDA device (``wf_paint3d``),
+        bit-identical to ``build()``: only the shell and bleed spheres cross
+        to the device."""
+        return self.material_map().build3d_device(device)
 
     def get_label(self) -> int:
         """0 healthy, 1 epidural, 2 subdural, 3 intracerebral (first bleed)."""

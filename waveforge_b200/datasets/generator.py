@@ -11,8 +11,8 @@ every receiver back with one host sync per element per step
 one batched FieldSet: one ``wf_fdtd3d_batch_run`` launch per step advances
 every member, each with its own transmitter, and the step kernel records
 all receivers.  Each member's signals are bit-identical to the reference's
-single solve; the phantom is painted once per sample instead of once per
-transmitter.  Sample dicts, ``.npz`` files and ``manifest.json`` keep the
+single solve; each phantom is painted once per sample on the GPU
+(``wf_paint3d``) instead of on the host once per transmitter.  Sample dicts, ``.npz`` files and ``manifest.json`` keep the
 reference's keys and layout (generator.py:386-428, :473-532).
 """
 
@@ -136,7 +136,7 @@ class BrainDatasetGenerator:
     def _run_simulation(self, phantom: BrainPhantom3D, tx_idx: int) -> tuple[np.ndarray, float]:
         """One transmitter: ((n_rx, n_steps) signals, Mcell-upd/s)
         (generator.py:162-224)."""
-        traces, mc = self._run_members([phantom.build()], [tx_idx])
+        traces, mc = self._run_members([phantom.build_device(self._device)], [tx_idx])
         self._ring.store(tx_idx, traces[0])
         return traces[0].cpu().numpy(), mc
 
@@ -144,7 +144,7 @@ class BrainDatasetGenerator:
         """Every transmitter of one phantom in one batched solve:
         ((n_tx, n_rx, n_steps) signals, Mcell-upd/s) (generator.py:226-248)."""
         self._ring.reset()
-        c = phantom.build()
+        c = phantom.build_device(self._device)
         traces, mc = self._run_members([c] * self._n_tx, list(range(self._n_tx)))
         for t in range(self._n_tx):
             self._ring.store(t, traces[t])
@@ -153,7 +153,7 @@ class BrainDatasetGenerator:
     def _run_pair(self, target: BrainPhantom3D, reference: BrainPhantom3D):
         """Both acquisitions of a sample (2 x n_tx solves) in one batched
         solve: (target signals, reference signals, Mcell-upd/s)."""
-        ct, cr = target.build(), reference.build()
+        ct, cr = target.build_device(self._device), reference.build_device(self._device)
         n = self._n_tx
         traces, mc = self._run_members([ct] * n + [cr] * n, list(range(n)) * 2)
         sig = traces.cpu().numpy()
