@@ -332,6 +332,13 @@ int32_t wf_paint2d(int32_t nx, int32_t ny, const wf_region2d* regions, int32_t n
                    float* ca, float* cb, double* eps_r, double* sigma,
                    int32_t* status, void* stream);
 
+/* Status of the 3D passes since the last call on this device, then cleared:
+ * 0, or WF_E_TIMEOUT when a bounded shared-memory pipeline wait of the TMA
+ * pass gave up (that column block stopped; its outputs are incomplete).
+ * Synchronous (reads a device word).  No reference counterpart: the
+ * reference has no device pipeline to wait on. */
+int32_t wf_fdtd3d_take_status(int32_t* status);
+
 /* One region of a painted 3D material map (painter's order: later regions
  * win), parameters float32-rounded as in wf_region2d
  * (MaterialMap3D, src/core/materials.py:297-423):

@@ -227,6 +227,11 @@ class FDTD3D(EngineBase):
                       f"field_max={self.last_field_max:.3e}  {self.mcells_per_second:.1f} Mcells/s")
         torch.cuda.synchronize(self._device)
         el = time.perf_counter() - t0
+        st = ctypes.c_int32(0)
+        nat.check(nat.load().wf_fdtd3d_take_status(ctypes.byref(st)))
+        if st.value:
+            raise RuntimeError(f"FDTD3D: a device pipeline wait gave up (status {st.value}); "
+                               "the fields of this run are incomplete")
         self.elapsed_time += el
         if el > 0:
             self.mcells_per_second = (self.steps_completed - start) * cells / el / 1e6

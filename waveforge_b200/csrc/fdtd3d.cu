@@ -780,6 +780,23 @@ static bool tma_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, i
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Status word of the TMA pass: a bounded mbarrier wait that gives up writes
+// WF_E_TIMEOUT here (and its CTA stops); wf_fdtd3d_take_status reads and
+// clears it.  Host code passes its device address, looked up once per device.
+static __device__ int g_tma_status;
+
+static int* tma_status_ptr() {
+  static int* ptr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  if (ptr[dev] == nullptr) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_tma_status) != cudaSuccess) return nullptr;
+    ptr[dev] = static_cast<int*>(p);
+  }
+  return ptr[dev];
+}
+
 // Opt k3d_tma into its dynamic shared memory (once per instantiation).
 template <bool MAT, bool FDIV>
 static int tma_attr() {
@@ -806,7 +823,8 @@ static int launch_tma(const TmaMaps& maps, const Tile3D& P, int seg_len, int n, 
   const int rc = tma_attr<MAT, FDIV>();
   if (rc != WF_OK) return rc;
   dim3 grid((unsigned)nblk, (unsigned)nb);
-  k3d_tma<MAT, FDIV><<<grid, kTJ * kTK, smem, st>>>(maps, P, tiles_j, tiles_k, seg_len, n, nullptr);
+  k3d_tma<MAT, FDIV><<<grid, kTJ * kTK, smem, st>>>(maps, P, tiles_j, tiles_k, seg_len, n,
+                                                     tma_status_ptr());
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "launch k3d_tma");
   return WF_OK;
@@ -1060,4 +1078,18 @@ extern "C" int32_t wf_fdtd3d_batch_run(const wf_grid3d* g, int32_t ninst, int64_
   return run3d(g, ninst, field_stride, coef_stride, trace_stride, src_stride, f, s, ca, cb, src,
                src_per_inst, probes, nprobe, traces, trace_ld, trace_step0, step0, nsteps,
                n_check, check_max, tune, stream);
+}
+
+extern "C" int32_t wf_fdtd3d_take_status(int32_t* status) {
+  if (status == nullptr) return set_error(WF_E_ARG, "wf_fdtd3d_take_status: null output");
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, wf::g_tma_status, sizeof(int));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyFromSymbol(status)");
+  if (v != 0) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(wf::g_tma_status, &zero, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(status)");
+  }
+  *status = v;
+  return WF_OK;
 }
