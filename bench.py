@@ -980,7 +980,7 @@ def main():
                        "dx_mm": 0.5, "courant": 0.5, "l2": "inputs > L2 (2.6 GB fields), no flush",
                        "batch_mode": batches[True].mode, "graph": args.graph,
                        "tune": args.tune if args.batch_mode != "auto" else
-                       [batches[True].depth, *batches[True].region],
+                       [batches[True].depth, *batches[True].region, batches[True].threads],
                        "parallelism": f"replicas x{ws}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},

@@ -263,6 +263,12 @@ class Batch2D:
     def depth(self) -> int:
         return 6 if self.tune is None else self.tune.steps_per_pass
 
+    @property
+    def threads(self) -> int:
+        """Threads per CTA of the register layout (1024: the 6-row layout of
+        the 48 x 128 region; 0: the region's default layout)."""
+        return 0 if self.tune is None else self.tune.threads
+
     def launches_per_run(self) -> int:
         """Kernel launches of one full ``run()``."""
         if self.mode == "persistent":

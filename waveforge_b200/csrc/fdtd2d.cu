@@ -60,16 +60,18 @@ __global__ void k_copy3(const float* __restrict__ a, const float* __restrict__ b
 wf_tune default_tune2d(int nx, int ny) {
   wf_tune t{};
   if ((long long)nx * ny >= 1024LL * 1024) {
+    // 48 x 128 regions on 1024 threads of 6 rows (two warps per 12-row
+    // column of the 512-thread layout): 159.9 vs 151.7 Gcell-upd/s at 4096^2
     t.steps_per_pass = 6;
     t.tile_i = 48;
     t.tile_j = 128;
+    t.threads = 1024;
   } else {
     t.steps_per_pass = 4;
     t.tile_i = 32;
     t.tile_j = 64;
   }
   t.tile_k = 1;
-  t.threads = 0;
   return t;
 }
 

@@ -7,6 +7,7 @@
 namespace wf {
 
 using Cfg48x128 = TileCfg<12, 4, 4>;  // 512 threads, 12 rows per thread
+using Cfg48x128w = TileCfg<6, 4, 8>;  // 1024 threads, 6 rows per thread (tune threads = 1024)
 using Cfg32x128 = TileCfg<16, 4, 2>;  // 256 threads, 16 rows per thread
 using Cfg32x64 = TileCfg<8, 2, 4>;    // 256 threads, 8 rows per thread
 using Cfg8x32 = TileCfg<4, 1, 2>;     // 64 threads (small grids and tests)
@@ -27,7 +28,8 @@ inline int check_tune2d(const wf_tune& t) {
 // Calls f.template operator()<Cfg>() for the configuration of t.
 template <class F>
 int dispatch_cfg2d(const wf_tune& t, const F& f) {
-  if (t.tile_i == 48) return f.template operator()<Cfg48x128>();
+  if (t.tile_i == 48)
+    return t.threads == 1024 ? f.template operator()<Cfg48x128w>() : f.template operator()<Cfg48x128>();
   if (t.tile_i == 32 && t.tile_j == 128) return f.template operator()<Cfg32x128>();
   if (t.tile_i == 32) return f.template operator()<Cfg32x64>();
   return f.template operator()<Cfg8x32>();

@@ -236,9 +236,14 @@ class Server:
         self.max_active = int(max_active_solves) if max_active_solves else 3 * nsm
         self.chunk = int(chunk_steps)
         self.max_wait_s = max_wait_s
-        self.tune = None if tune is None else nat.WfTune(*tune)
-        self.depth = 6 if self.tune is None else self.tune.steps_per_pass
-        self.region = (48, 128) if self.tune is None else (self.tune.tile_i, self.tune.tile_j)
+        # default: tiled -- depth 4 on 48 x 128 regions of the 1024-thread
+        # layout (the fastest served throughput on the Poisson stream of mixed
+        # sides); persistent -- depth 6 on the 512-thread layout
+        if tune is None:
+            tune = (4, 48, 128, 1, 1024) if mode == "tiled" else (6, 48, 128, 1, 0)
+        self.tune = nat.WfTune(*tune)
+        self.depth = self.tune.steps_per_pass
+        self.region = (self.tune.tile_i, self.tune.tile_j)
         self.ctas_per_sm = ctas_per_sm
         self.stream = torch.cuda.current_stream(self.device)
         self.side = torch.cuda.Stream(self.device)
@@ -394,7 +399,7 @@ class Server:
             self._queue_ctr.zero_()
             nat.check(nat.load().wf_batch2d_run(
                 dev.data_ptr(), nsol, dev.data_ptr() + nsol * dsz, self._queue_ctr.data_ptr(),
-                None if self.tune is None else ctypes.byref(self.tune), self.ctas_per_sm,
+                ctypes.byref(self.tune), self.ctas_per_sm,
                 1 if fast else 0, stream))
             self.launches += 1
         else:
