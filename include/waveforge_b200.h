@@ -94,7 +94,8 @@ typedef struct wf_probe {
  * block depth K.  2D: tile_i x tile_j = the on-chip REGION of one CTA
  * (core + K-cell halo on each side); it selects one of the compiled
  * register layouts: 48x128 (512 threads, 12 rows each; threads = 1024 selects
- * the same region on 1024 threads of 6 rows), 32x128, 32x64 (256), 8x32 (64).
+ * the same region on 1024 threads of 6 rows), 64x128 (1024 threads of 8 rows),
+ * 32x128, 32x64 (256), 8x32 (64).
  * 3D: tile_i x tile_j x tile_k = core cells per CTA, threads per CTA; with
  * tile_i = 0 the streaming kernels (tile_j = segment length, threads = variant). */
 typedef struct wf_tune {

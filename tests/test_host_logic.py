@@ -31,7 +31,8 @@ def test_pass_plan_covers_steps_and_lands_in_state(K):
             assert all(x == 1 for x in lens)
 
 
-@pytest.mark.parametrize("region,k", [((48, 128), 6), ((32, 64), 3), ((8, 32), 1), ((32, 128), 4)])
+@pytest.mark.parametrize("region,k", [((48, 128), 6), ((64, 128), 8), ((32, 64), 3), ((8, 32), 1),
+                                      ((32, 128), 4)])
 def test_tile_items_partition_every_grid(region, k):
     rng = np.random.default_rng(3)
     shapes = [tuple(int(v) for v in rng.integers(4, 300, 2)) for _ in range(5)]

@@ -28,7 +28,8 @@ pytestmark = pytest.mark.gpu
 # layout, with temporal-block depths from 1 to the largest that leaves a core
 TUNES = [None, (1, 8, 32, 1, 0), (2, 8, 32, 1, 0), (3, 8, 32, 1, 0), (4, 32, 64, 1, 0),
          (7, 32, 64, 1, 0), (5, 32, 128, 1, 0), (6, 48, 128, 1, 0), (11, 48, 128, 1, 0),
-         (4, 48, 128, 1, 1024), (1, 48, 128, 1, 1024), (9, 48, 128, 1, 1024)]
+         (4, 48, 128, 1, 1024), (1, 48, 128, 1, 1024), (9, 48, 128, 1, 1024),
+         (6, 64, 128, 1, 1024), (13, 64, 128, 1, 1024)]
 
 
 def sim2d(cuda, nx, ny, dx, courant, sources_spec, ca=None, cb=None, steps=None, tune=None,
@@ -146,7 +147,7 @@ def test_breast_mimo_alone_and_batched_bit_exact(cuda):
             keys.append(f"p{p}_tx{tx}")
     for mode in ("persistent", "tiled"):
         for tune in (None, (3, 32, 64, 1, 0), (6, 48, 128, 1, 0), (2, 8, 32, 1, 0),
-                     (4, 48, 128, 1, 1024), (5, 48, 128, 1, 1024)):
+                     (4, 48, 128, 1, 1024), (5, 48, 128, 1, 1024), (7, 64, 128, 1, 1024)):
             batch = Batch2D(solves, steps, tune=tune, mode=mode)
             if mode == "tiled":
                 for chunk in (7, 100, 1, steps - 108):   # uneven chunks, a single-step pass

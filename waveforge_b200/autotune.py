@@ -28,10 +28,14 @@ BATCH_CANDIDATES = (
     # the same 48 x 128 region on 1024 threads of 6 rows (64 registers: twice the warps)
     ("tiled", (4, 48, 128, 1, 1024)), ("tiled", (5, 48, 128, 1, 1024)),
     ("tiled", (6, 48, 128, 1, 1024)),
+    # 64 x 128 regions on 1024 threads of 8 rows: less halo, deeper passes
+    ("tiled", (6, 64, 128, 1, 1024)), ("tiled", (7, 64, 128, 1, 1024)),
+    ("tiled", (8, 64, 128, 1, 1024)),
 )
 PLAIN_CANDIDATES = ((4, 48, 128, 1, 0), (6, 48, 128, 1, 0), (8, 48, 128, 1, 0),
                     (4, 32, 64, 1, 0), (4, 32, 128, 1, 0), (2, 32, 64, 1, 0),
-                    (4, 48, 128, 1, 1024), (5, 48, 128, 1, 1024), (6, 48, 128, 1, 1024))
+                    (4, 48, 128, 1, 1024), (5, 48, 128, 1, 1024), (6, 48, 128, 1, 1024),
+                    (6, 64, 128, 1, 1024), (8, 64, 128, 1, 1024))
 
 _cache: dict = {}
 

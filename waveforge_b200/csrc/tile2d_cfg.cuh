@@ -8,17 +8,18 @@ namespace wf {
 
 using Cfg48x128 = TileCfg<12, 4, 4>;  // 512 threads, 12 rows per thread
 using Cfg48x128w = TileCfg<6, 4, 8>;  // 1024 threads, 6 rows per thread (tune threads = 1024)
+using Cfg64x128w = TileCfg<8, 4, 8>;  // 1024 threads, 8 rows per thread (64 registers)
 using Cfg32x128 = TileCfg<16, 4, 2>;  // 256 threads, 16 rows per thread
 using Cfg32x64 = TileCfg<8, 2, 4>;    // 256 threads, 8 rows per thread
 using Cfg8x32 = TileCfg<4, 1, 2>;     // 64 threads (small grids and tests)
 
 inline int check_tune2d(const wf_tune& t) {
   const int rh = t.tile_i, rw = t.tile_j, k = t.steps_per_pass;
-  const bool known = (rh == 48 && rw == 128) || (rh == 32 && rw == 128) ||
+  const bool known = (rh == 48 && rw == 128) || (rh == 64 && rw == 128) || (rh == 32 && rw == 128) ||
                      (rh == 32 && rw == 64) || (rh == 8 && rw == 32);
   if (!known)
     return set_error(WF_E_ARG,
-                     "2D tune: region %dx%d is not compiled (48x128, 32x128, 32x64, 8x32)", rh,
+                     "2D tune: region %dx%d is not compiled (48x128, 64x128, 32x128, 32x64, 8x32)", rh,
                      rw);
   if (k < 1 || 2 * k >= rh || 2 * k >= rw)
     return set_error(WF_E_ARG, "2D tune: k=%d leaves no core in a %dx%d region", k, rh, rw);
@@ -30,6 +31,7 @@ template <class F>
 int dispatch_cfg2d(const wf_tune& t, const F& f) {
   if (t.tile_i == 48)
     return t.threads == 1024 ? f.template operator()<Cfg48x128w>() : f.template operator()<Cfg48x128>();
+  if (t.tile_i == 64) return f.template operator()<Cfg64x128w>();
   if (t.tile_i == 32 && t.tile_j == 128) return f.template operator()<Cfg32x128>();
   if (t.tile_i == 32) return f.template operator()<Cfg32x64>();
   return f.template operator()<Cfg8x32>();
