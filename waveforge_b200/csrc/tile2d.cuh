@@ -69,9 +69,9 @@ struct TileCfg {
 // Shared memory of the tile routine (sized for the configuration).
 template <class C>
 struct TileSmem {
-  float xe[C::RH][C::WX];   // Ex of each warp column's lane 0 (for lane 31 of the left warp)
+  alignas(16) float xe[C::WX][C::RH];  // Ex of each warp column's lane 0 (for lane 31 of the left warp)
   float yr[C::WY][C::RW];   // Ey of each segment's first row (for the segment above)
-  float hx[C::RH][C::WX];   // Hz of each warp column's lane 31 (for lane 0 of the right warp)
+  alignas(16) float hx[C::WX][C::RH];  // Hz of each warp column's lane 31 (for lane 0 of the right warp)
   float hr[C::WY][C::RW];   // Hz of each segment's last row (for the segment below)
   float sp[C::RH][C::RW];   // Mur staging: pre-step Hz
   float sc[C::RH][C::RW];   // Mur staging: curl-updated Hz
@@ -81,6 +81,25 @@ struct TileSmem {
   short p[kMaxLocalProbe];
   unsigned bmax[3];
 };
+
+// Store a thread's R consecutive rows into a shared row of R floats with the
+// widest aligned vector stores (16-byte when R % 4 == 0, else 8-byte when R
+// is even): one lane writes a warp column's boundary values in R/4 or R/2
+// instructions instead of R.
+template <int R>
+__device__ __forceinline__ void store_rows(float* dst, const float (&v)[R]) {
+  if constexpr (R % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < R; q += 4)
+      *reinterpret_cast<float4*>(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+  } else if constexpr (R % 2 == 0) {
+#pragma unroll
+    for (int q = 0; q < R; q += 2) *reinterpret_cast<float2*>(dst + q) = make_float2(v[q], v[q + 1]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst[q] = v[q];
+  }
+}
 
 // Value of wave * amp for cell (i,j) of source s (row-major box offset).
 __device__ __forceinline__ float src_value(const wf_source& s, int i, int j, int n) {
@@ -136,10 +155,7 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
       }
     }
     // exchange for the Faraday update
-    if (lane == 0) {
-#pragma unroll
-      for (int q = 0; q < R; ++q) S.xe[r0 + q][wx] = ex[q];
-    }
+    if (lane == 0) store_rows<R>(&S.xe[wx][r0], ex);
     S.yr[wy][c] = ey[0];
     __syncthreads();
 
@@ -147,7 +163,7 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       float exr = __shfl_down_sync(0xffffffffu, ex[q], 1);
-      if (lane == 31) exr = (wx + 1 < WX) ? S.xe[r0 + q][wx + 1] : 0.f;
+      if (lane == 31) exr = (wx + 1 < WX) ? S.xe[wx + 1][r0 + q] : 0.f;
       float eyb;
       if (q + 1 < R) eyb = ey[q + 1];
       else eyb = (wy + 1 < WY) ? S.yr[wy + 1][c] : 0.f;
@@ -201,10 +217,7 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
     }
 
     // exchange for the Ampere update
-    if (lane == 31) {
-#pragma unroll
-      for (int q = 0; q < R; ++q) S.hx[r0 + q][wx] = hz[q];
-    }
+    if (lane == 31) store_rows<R>(&S.hx[wx][r0], hz);
     S.hr[wy][c] = hz[R - 1];
     __syncthreads();
 
@@ -212,7 +225,7 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       float hl = __shfl_up_sync(0xffffffffu, hz[q], 1);
-      if (lane == 0) hl = (wx > 0) ? S.hx[r0 + q][wx - 1] : 0.f;
+      if (lane == 0) hl = (wx > 0) ? S.hx[wx - 1][r0 + q] : 0.f;
       float ha;
       if (q > 0) ha = hz[q - 1];
       else ha = (wy > 0) ? S.hr[wy - 1][c] : 0.f;
