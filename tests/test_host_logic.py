@@ -127,3 +127,22 @@ def test_no_cpu_fallback():
     mm = MaterialMap(g).add_circle((8.0, 8.0), 3.0, Material("d", 4.0, 0.0))
     with pytest.raises(RuntimeError, match="CUDA"):
         mm.build_device("cpu")
+
+
+def test_dataset_cli_dry_run_and_arguments(capsys):
+    """The generator's command line keeps the reference's arguments
+    (datasets/generate_brain_dataset.py:60-108); --dry_run exits 0 without a GPU."""
+    from waveforge_b200.datasets import generate_brain_dataset as cli
+    a = cli.parse_args(["--n_samples", "8", "--output_dir", "/tmp/x", "--phantom", "B",
+                        "--freq_low_ghz", "1", "--freq_high_ghz", "3", "--grid_size", "48"])
+    assert (a.n_samples, a.phantom, a.grid_size, a.n_tx, a.ring_radius, a.n_steps) == (8, "B", 48, 8, 30, 300)
+    assert cli.main(["--n_samples", "4", "--output_dir", "/tmp/x", "--dry_run"]) == 0
+    assert "DRY RUN" in capsys.readouterr().out
+
+
+def test_cole_cole_spectrum_matches_pointwise():
+    from waveforge_b200.datasets.brain import TISSUES, cole_cole_spectrum, cole_cole_to_fdtd
+    f, e, s = cole_cole_spectrum(TISSUES["gray_matter"], 1e8, 1e10, 7)
+    for x, ee, ss in zip(f, e, s):
+        assert (ee, ss) == cole_cole_to_fdtd(TISSUES["gray_matter"], float(x))
+    assert e[0] > e[-1] and s[0] < s[-1]   # dispersion: permittivity falls, loss rises
