@@ -655,7 +655,7 @@ def bench_dataset(args, ws, rank, local):
         i = next(counter)
         smp = gen.generate_sample(label=i % 4, seed=args.seed * 1000 + i)
         if smp is not None:
-            gen.save_sample(smp, i)
+            gen.save_sample_async(smp, i)   # written while the next sample solves
         return smp
 
     def plain():
@@ -673,6 +673,7 @@ def bench_dataset(args, ws, rank, local):
 
     for _ in range(args.warmup):
         one()
+    gen.flush()
     torch.cuda.synchronize(dev)
     barrier(ws)
     clk = ClockSampler(local)
@@ -681,6 +682,7 @@ def bench_dataset(args, ws, rank, local):
     done = 0
     for _ in range(args.steps):
         done += one() is not None
+    gen.flush()
     torch.cuda.synchronize(dev)
     el = time.perf_counter() - t0
     clocks = clk.stop()

@@ -22,6 +22,7 @@ import json
 import math
 import random
 import time
+from concurrent.futures import Future, ThreadPoolExecutor
 from pathlib import Path
 from typing import Optional
 
@@ -233,6 +234,23 @@ class BrainDatasetGenerator:
             "_mcells_per_second": np.float32(mc),
         }
 
+    def save_sample_async(self, sample: dict, sample_idx: int) -> Future:
+        """``save_sample`` on a background writer thread (zlib compression
+        releases the GIL, so the next sample's solve overlaps the write);
+        ``flush()`` waits for every pending write."""
+        if getattr(self, "_writer", None) is None:
+            self._writer = ThreadPoolExecutor(max_workers=1)
+            self._pending: list = []
+        fut = self._writer.submit(self.save_sample, sample, sample_idx)
+        self._pending.append(fut)
+        return fut
+
+    def flush(self) -> list:
+        """Wait for the pending background writes; returns their paths."""
+        done = [f.result() for f in getattr(self, "_pending", [])]
+        self._pending = []
+        return done
+
     def save_sample(self, sample: dict, sample_idx: int) -> Path:
         """``sample_<idx:06d>.npz`` (compressed): every array and numpy
         scalar, plus the string fields as 0-d arrays (generator.py:418-428)."""
@@ -270,7 +288,8 @@ class BrainDatasetGenerator:
                 if show_progress:
                     print(f"  [{i + 1}/{n_samples}] SKIP (bleed placement failed, label={label})")
                 continue
-            path = self.save_sample(sample, idx)
+            path = self._output_dir / f"sample_{idx:06d}.npz"
+            self.save_sample_async(sample, idx)
             manifest["n_completed"] += 1
             manifest["class_counts"][int(label)] += 1
             manifest["sample_paths"].append(str(path))
@@ -285,6 +304,7 @@ class BrainDatasetGenerator:
                       f"age={sample['bleed_age']:9} {float(sample['_mcells_per_second']):.1f}Mc/s "
                       f"ETA:{eta / 60:.0f}min")
             idx += 1
+        self.flush()
         path = self._output_dir / "manifest.json"
         with open(path, "w") as fh:
             json.dump(manifest, fh, indent=2)
