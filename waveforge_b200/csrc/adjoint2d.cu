@@ -94,11 +94,13 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj2d_step(Adj2D A, int tiles_j
     const int i = i0 + r, j = j0 + c;
     float ax = 0.f, ay = 0.f, ah = 0.f, b = 0.f;
     if (inside(i, j)) {
+      // read-only for the whole launch: non-coherent loads the compiler may
+      // issue together
       const long long g = (long long)i * ny + j;
-      ax = A.lin[0][g];
-      ay = A.lin[1][g];
-      ah = A.lin[2][g];
-      b = MAT ? A.cb[g] : A.de;
+      ax = __ldg(&A.lin[0][g]);
+      ay = __ldg(&A.lin[1][g]);
+      ah = __ldg(&A.lin[2][g]);
+      b = MAT ? __ldg(&A.cb[g]) : A.de;
     }
     sEx[r][c] = ax;
     sEy[r][c] = ay;
@@ -172,12 +174,31 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj2d_step(Adj2D A, int tiles_j
     const int i = i0 + r, j = j0 + c;
     return (i >= 0 && i < nx - 1 && j >= 0 && j < ny - 1) ? A.dh * sB[r][c] : 0.f;
   };
+#pragma unroll 2
   for (int q = tid; q < kAdjTI * kAdjTJ; q += kAdjThreads) {
     const int rr = q / kAdjTJ, cc = q - rr * kAdjTJ;
     const int r = rr + kAdjHalo, c = cc + kAdjHalo;
     const int i = i0 + r, j = j0 + c;
     if (!inside(i, j)) continue;
     const long long g = (long long)i * ny + j;
+    // every global input of the cell first (the stores below could alias
+    // plain loads issued after them); the accumulators belong to this cell only
+    const float ca = MAT ? __ldg(&A.ca[g]) : 1.f;
+    float h = 0.f, hjm = 0.f, him = 0.f, exn = 0.f, eyn = 0.f;
+    double gca0 = 0.0, gcb0 = 0.0;
+    if (MAT) {
+      h = __ldg(&A.hz_n1[g]);
+      if (j >= 1) {
+        hjm = __ldg(&A.hz_n1[g - 1]);
+        exn = __ldg(&A.ex_n[g]);
+      }
+      if (i >= 1) {
+        him = __ldg(&A.hz_n1[g - ny]);
+        eyn = __ldg(&A.ey_n[g]);
+      }
+      gca0 = A.gca[g];
+      gcb0 = A.gcb[g];
+    }
     // adjoint of the Mur snapshot hp (pre-injection Hz)
     float ahp = 0.f;
     if (j == 1) ahp += sY[r][c - 1];
@@ -189,7 +210,6 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj2d_step(Adj2D A, int tiles_j
     if (i == nx - 2) ahp += sH[r + 1][c];
     if (i == nx - 1) ahp -= A.mx * sH[r][c];
     const float aex1 = sEx[r][c], aey1 = sEy[r][c];
-    const float ca = MAT ? A.ca[g] : 1.f;
     const float aex = (j >= 1 ? ca * aex1 : aex1) + (pf(r, c - 1) - pf(r, c)) * A.rdy;
     const float aey = (i >= 1 ? ca * aey1 : aey1) + (pf(r, c) - pf(r - 1, c)) * A.rdx;
     A.lout[0][g] = aex;
@@ -197,17 +217,16 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj2d_step(Adj2D A, int tiles_j
     A.lout[2][g] = sB[r][c] + ahp;
     if (MAT) {
       double gca = 0.0, gcb = 0.0;
-      const float h = A.hz_n1[g];
       if (j >= 1) {
-        gca += (double)aex1 * (double)A.ex_n[g];
-        gcb += (double)aex1 * ((double)(h - A.hz_n1[g - 1]) * (double)A.rdy);
+        gca += (double)aex1 * (double)exn;
+        gcb += (double)aex1 * ((double)(h - hjm) * (double)A.rdy);
       }
       if (i >= 1) {
-        gca += (double)aey1 * (double)A.ey_n[g];
-        gcb -= (double)aey1 * ((double)(h - A.hz_n1[g - ny]) * (double)A.rdx);
+        gca += (double)aey1 * (double)eyn;
+        gcb -= (double)aey1 * ((double)(h - him) * (double)A.rdx);
       }
-      A.gca[g] += gca;
-      A.gcb[g] += gcb;
+      A.gca[g] = gca0 + gca;
+      A.gcb[g] = gcb0 + gcb;
     }
   }
 }
