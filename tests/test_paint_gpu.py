@@ -130,3 +130,26 @@ def test_device_painter_3d_rejects_custom_masks(cuda):
     assert not mm.device_paintable3d
     with pytest.raises(ValueError):
         mm.build3d_device(cuda)
+
+
+def test_device_painter_3d_reports_bad_material_index(cuda):
+    """A region whose material index is outside the table paints the default
+    and sets the status word (no fault)."""
+    import ctypes
+    from waveforge_b200 import _native as nat
+    lib = nat.load()
+    regs = (nat.WfRegion3D * 1)()
+    regs[0].kind, regs[0].material = 0, 5          # table holds 2 materials
+    for t, v in enumerate((3.0, 3.0, 3.0, 4.0)):
+        regs[0].p[t] = v
+    host = torch.frombuffer(bytearray(bytes(memoryview(regs).cast("B"))), dtype=torch.uint8)
+    dreg = host.to(cuda)
+    tca = torch.tensor([0.5, 0.25], device=cuda)
+    tcb = torch.tensor([1.0, 2.0], device=cuda)
+    ca = torch.zeros((6, 6, 6), device=cuda)
+    cb = torch.zeros_like(ca)
+    st = torch.zeros(1, dtype=torch.int32, device=cuda)
+    nat.check(lib.wf_paint3d(6, 6, 6, dreg.data_ptr(), 1, tca.data_ptr(), tcb.data_ptr(), 2,
+                             ca.data_ptr(), cb.data_ptr(), st.data_ptr(), nat.stream_handle(cuda)))
+    assert int(st.item()) == nat.WF_E_ARG
+    assert torch.all(ca == 0.5) and torch.all(cb == 1.0)

@@ -182,3 +182,54 @@ def test_batched_instances_equal_separate_runs(cuda):
         maxima.append(s1.last_field_max)
     assert sim.last_field_max == max(maxima)
     assert float(tr.abs().max()) > 0
+
+
+@pytest.mark.parametrize("nz", [40, 39])
+def test_member_sources_equal_separate_runs(cuda, nz):
+    """FDTD3D(member_sources=...): each batch member injects its own sources
+    (here a different transmitter and waveform per member) and equals the
+    separate single run bit for bit -- on the TMA pass (Nz % 4 == 0) and on
+    the register streaming kernel it falls back to otherwise."""
+    from waveforge_b200 import FieldSet as FS
+    rng = np.random.default_rng(31 + nz)
+    B, steps = 4, 14
+    shape = (21, 30, nz)
+    ca = torch.from_numpy(rng.uniform(0.3, 1.0, shape).astype(np.float32))
+    cb = torch.from_numpy(rng.uniform(0.001, 0.1, shape).astype(np.float32))
+    waves = [torch.from_numpy(rng.standard_normal(steps).astype(np.float32)) for _ in range(B)]
+    pos = [(5, 7, 9), (15, 20, 30), (10, 3, 2), (19, 28, nz - 2)]
+    probes = [("Ez", 10, 15, 20), ("Hy", 3, 28, 1), ("Ex", 20, 1, nz - 1)]
+    g = YeeGrid(*shape[:2], 1e-3, 1e-3, Nz=nz, dz=1e-3, courant=0.9, device=cuda)
+    f = FS(g, batch_size=B)
+    members = [SourceCollection([PointSource(TabulatedWaveform(waves[b]), *pos[b][:2], "Ez",
+                                             k=pos[b][2], grid=g, N_steps=steps)]) for b in range(B)]
+    sim = FDTD3D(g, f, MurABC3D(g, f.Hx, f.Hy, f.Hz), Ca=ca.to(cuda), Cb=cb.to(cuda),
+                 member_sources=members)
+    tr = sim.run(steps, record=Detectors(probes)).cpu()
+    for b in range(B):
+        i, j, k = pos[b]
+        s1, f1 = sim3d(cuda, shape, 1e-3, 0.9, [("Ez", (i, i + 1, j, j + 1, k, k + 1), waves[b])],
+                       ca, cb, steps=steps)
+        assert torch.equal(s1.run(steps, record=Detectors(probes)).cpu(), tr[b]), b
+        for c in COMPS:
+            assert torch.equal(getattr(f1, c).cpu(), getattr(f, c)[b].cpu()), (b, c)
+
+
+def test_member_sources_validation(cuda):
+    from waveforge_b200 import FieldSet as FS, LineSource
+    g = YeeGrid(12, 12, 1e-3, 1e-3, Nz=12, dz=1e-3, courant=0.9, device=cuda)
+    w = TabulatedWaveform(torch.ones(4))
+    one = SourceCollection([PointSource(w, 3, 3, "Ez", k=3, grid=g, N_steps=4)])
+    two = SourceCollection([PointSource(w, 3, 3, "Ez", k=3, grid=g, N_steps=4),
+                            PointSource(w, 5, 5, "Ez", k=5, grid=g, N_steps=4)])
+    f = FS(g, batch_size=2)
+    b = MurABC3D(g, f.Hx, f.Hy, f.Hz)
+    with pytest.raises(ValueError):
+        FDTD3D(g, FS(g), MurABC3D(g, f.Hx, f.Hy, f.Hz), member_sources=[one])  # not batched
+    with pytest.raises(ValueError):
+        FDTD3D(g, f, b, member_sources=[one])                                  # wrong count
+    with pytest.raises(ValueError):
+        FDTD3D(g, f, b, one, member_sources=[one, one])                        # both kinds
+    sim = FDTD3D(g, f, b, member_sources=[one, two])                           # box counts differ
+    with pytest.raises(ValueError):
+        sim.run(2)
