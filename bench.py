@@ -31,6 +31,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -140,8 +141,10 @@ class ClockSampler:
 
     def start(self):
         try:
-            out_dir = ROOT / "gpurun_out"
-            out_dir.mkdir(exist_ok=True)
+            # raw samples go to WAVEFORGE_B200_CLOCKS_DIR (default: the temp
+            # dir); the JSON line carries their summary
+            out_dir = Path(os.environ.get("WAVEFORGE_B200_CLOCKS_DIR", tempfile.gettempdir()))
+            out_dir.mkdir(parents=True, exist_ok=True)
             self.path = out_dir / f"clocks_gpu{self.gpu}.csv"
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
