@@ -335,6 +335,25 @@ int32_t wf_paint2d(int32_t nx, int32_t ny, const wf_region2d* regions, int32_t n
                    float* ca, float* cb, double* eps_r, double* sigma,
                    int32_t* status, void* stream);
 
+/* 2D TM leapfrog with a convolutional PML of `depth` cells on every side in
+ * place of the Mur edges.  No reference counterpart: the reference only
+ * stores the graded profiles (src/core/boundaries.py:32-112, MurABC
+ * pml_depth) and never applies them.  Arguments as wf_fdtd2d_run (fields
+ * updated in place, no scratch), plus
+ *  tables  6*(nx+ny) float32 on the device: for the x axis (nx entries each)
+ *          b_E, c_E, 1/kappa_E, b_H, c_H, 1/kappa_H, then the same for y;
+ *          E samples at integer cells, H samples at half cells
+ *  psi     4*depth*(nx+ny) float32 on the device (zero before the first
+ *          step): Hz-x [2*depth][ny], Ey-x [2*depth][ny], Hz-y [nx][2*depth],
+ *          Ex-y [nx][2*depth] layer memories, updated in place.
+ * Outside the layers the update is the reference's, bit for bit. */
+int32_t wf_cpml2d_run(const wf_grid2d* g, float* ex, float* ey, float* hz, const float* ca,
+                      const float* cb, int32_t depth, const float* tables, float* psi,
+                      const wf_source* src, int32_t nsrc, const wf_probe* probes,
+                      int32_t nprobe, float* traces, int64_t trace_ld, int32_t trace_step0,
+                      int32_t step0, int32_t nsteps, int32_t n_check, uint32_t* check_max,
+                      void* stream);
+
 /* Status of the 3D passes since the last call on this device, then cleared:
  * 0, or WF_E_TIMEOUT when a bounded shared-memory pipeline wait of the TMA
  * pass gave up (that column block stopped; its outputs are incomplete).

@@ -13,14 +13,14 @@ from .sources import (
     PointSource, RickerWavelet, SinusoidalSource, SourceCollection, TabulatedWaveform, UWBPulse,
     Waveform,
 )
-from .boundaries import MurABC, MurABC3D
+from .boundaries import CPML, MurABC, MurABC3D
 from .fdtd2d import FDTD2D, SimulationDivergedError
 from .fdtd3d import FDTD3D
 
 __all__ = [
     "C0", "Chirp", "FDTD2D", "FDTD3D", "FIELD_COMPONENTS", "FieldSet", "GaussianDerivativePulse",
     "GaussianPulse", "GridMetadata", "LineSource", "Material", "MaterialMap", "MaterialMap3D",
-    "ModulatedGaussian", "MurABC", "MurABC3D", "PlaneSource", "PointSource", "RickerWavelet",
+    "ModulatedGaussian", "MurABC", "MurABC3D", "CPML", "PlaneSource", "PointSource", "RickerWavelet",
     "SimulationDivergedError", "SinusoidalSource", "SourceCollection", "StaggerOffset",
     "TISSUE_LIBRARY", "TabulatedWaveform", "UWBPulse", "Waveform", "YEE_OFFSETS", "YeeGrid",
     "compute_stable_dt",

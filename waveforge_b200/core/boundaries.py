@@ -169,3 +169,67 @@ class MurABC3D:
         return (f"MurABC3D(shape=({self._Nx}, {self._Ny}, {self._Nz}), C_mur_x={self.C_mur_x:.6f}, "
                 f"C_mur_y={self.C_mur_y:.6f}, C_mur_z={self.C_mur_z:.6f}, "
                 f"n_boundary_cells={self.n_boundary_cells})")
+
+
+class CPML:
+    """Convolutional PML of ``depth`` cells on every side of a 2D TM grid, for
+    ``FDTD2D(grid, fields, CPML(grid, depth), ...)`` in place of ``MurABC``.
+
+    New: the reference computes these graded profiles (``_compute_pml_coeffs``,
+    src/core/boundaries.py:32-112, stored by ``MurABC(pml_depth=...)``) but no
+    engine applies them, so ``MurABC(pml_depth=...)`` keeps the reference's
+    Mur behaviour and this separate class runs the layer.  Same profile
+    (cubic grading, R = 1e-8, kappa_max = 5, alpha_max = 0.05 by default);
+    the coefficients (b, c, 1/kappa) are sampled at every position of each
+    axis -- integer cells for the E updates, half cells for Hz -- at depth
+    rho = (D - x) / D on the low side and (x - (n - 1 - D)) / D on the high
+    side.  ``psi`` holds the layers' convolution memories (4 D (Nx + Ny)
+    floats) and is zeroed by ``reset``."""
+
+    is_cpml = True
+
+    def __init__(self, grid: YeeGrid, depth: int = 10, *, R: float = 1e-8, m: int = 3,
+                 kappa_max: float = 5.0, alpha_max: float = 0.05) -> None:
+        if grid.Nz != 1:
+            raise ValueError("CPML is implemented for 2D grids (Nz = 1)")
+        if depth < 1 or 2 * depth + 2 > min(grid.Nx, grid.Ny):
+            raise ValueError(f"a {depth}-cell layer per side does not fit a "
+                             f"{grid.Nx}x{grid.Ny} grid")
+        self._Nx, self._Ny = grid.Nx, grid.Ny
+        self.depth = depth
+        self._params = (R, m, kappa_max, alpha_max)
+        dt = grid.dt
+        tx = self.profile(grid.Nx, grid.dx, dt)
+        ty = self.profile(grid.Ny, grid.dy, dt)
+        self.tables = torch.tensor(tx + ty, dtype=torch.float32).to(grid.device)
+        self.psi = torch.zeros(4 * depth * (grid.Nx + grid.Ny), dtype=torch.float32,
+                               device=grid.device)
+
+    def profile(self, n: int, d: float, dt: float) -> list:
+        """[b_E, c_E, 1/kappa_E, b_H, c_H, 1/kappa_H] over the n positions of
+        one axis (float64, rounded to float32 by the caller); positions
+        outside the layer read as (1, 0, 1)."""
+        R, m, kmax, amax = self._params
+        D = self.depth
+        smax = (m + 1) * math.log(1.0 / R) / (2.0 * ETA0 * D * d)
+        out = [[], [], [], [], [], []]
+        for half, base in ((0.0, 0), (0.5, 3)):
+            for i in range(n):
+                x = i + half
+                rho = max((D - x) / D, (x - (n - 1 - D)) / D, 0.0)
+                if rho <= 0.0 or (half and i > n - 2):
+                    b, c, ik = 1.0, 0.0, 1.0
+                else:
+                    rho = min(rho, 1.0)
+                    _, b, c = _pml_bsigma_at_rho(rho, smax, kmax, amax, m, dt)
+                    ik = 1.0 / (1.0 + (kmax - 1.0) * rho ** m)
+                out[base].append(b)
+                out[base + 1].append(c)
+                out[base + 2].append(ik)
+        return [v for col in out for v in col]
+
+    def reset(self) -> None:
+        self.psi.zero_()
+
+    def __repr__(self) -> str:
+        return f"CPML(grid=({self._Nx}, {self._Ny}), depth={self.depth})"

@@ -62,9 +62,14 @@ class FDTD2D(EngineBase):
             nat.require_cuda(Ca, "Ca")
             nat.require_cuda(Cb, "Cb")
         nat.load()
+        # a CPML boundary (new) replaces the Mur edges: the step runs wf_cpml2d_run
+        self._cpml = bool(getattr(boundary, "is_cpml", False))
+        if self._cpml and fields.is_batched:
+            raise ValueError("the CPML engine runs unbatched FieldSets")
+        mx = 0.0 if self._cpml else boundary.C_mur_x
+        my = 0.0 if self._cpml else boundary.C_mur_y
         self._g = nat.WfGrid2D(grid.Nx, grid.Ny, nat.f32(self._Dh), nat.f32(self._De),
-                               nat.f32(grid.dx), nat.f32(grid.dy),
-                               nat.f32(boundary.C_mur_x), nat.f32(boundary.C_mur_y),
+                               nat.f32(grid.dx), nat.f32(grid.dy), nat.f32(mx), nat.f32(my),
                                nat.fastdiv_flags(self._device, grid.dx, grid.dy))
         self._tune = tune_struct(tune)
         self._scratch: Optional[torch.Tensor] = None
@@ -103,6 +108,18 @@ class FDTD2D(EngineBase):
             for t in (ex, ey, hz) + ((ca, cb) if ca is not None else ()):
                 if not t.is_contiguous() or t.numel() != g.Nx * g.Ny:
                     raise ValueError("field / coefficient tensors must be contiguous (Nx, Ny, 1)")
+            if self._cpml:
+                bd = self._boundary
+                nat.check(lib.wf_cpml2d_run(
+                    ctypes.byref(self._g), ex.data_ptr(), ey.data_ptr(), hz.data_ptr(),
+                    nat.ptr(ca), nat.ptr(cb), bd.depth, bd.tables.data_ptr(), bd.psi.data_ptr(),
+                    src.ptr, src.count, None if probes is None else probes.ptr,
+                    0 if probes is None else probes.count,
+                    None if traces is None else traces.data_ptr(),
+                    0 if traces is None else traces.stride(0), step0, step0, nsteps,
+                    self._n_check if chk is not None else 0,
+                    None if chk is None else chk.data_ptr(), stream))
+                continue
             s = self._scratch
             nat.check(lib.wf_fdtd2d_run(
                 ctypes.byref(self._g), ex.data_ptr(), ey.data_ptr(), hz.data_ptr(),
@@ -116,6 +133,12 @@ class FDTD2D(EngineBase):
                 None if self._tune is None else ctypes.byref(self._tune), stream))
         self.steps_completed += nsteps
         self._process_checks(chk, count, step0)
+
+    def reset(self) -> None:
+        """Zero fields and telemetry, and the CPML layer memories if any."""
+        super().reset()
+        if self._cpml:
+            self._boundary.reset()
 
     # ------------------------------------------------------------------
     def step(self) -> None:
