@@ -455,8 +455,18 @@ def bench_single(args, ws, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = bpc * upd / (ms_step * 1e-3) / 1e9
     k = sim._tune.steps_per_pass if sim._tune is not None else None
+    # DRAM bytes of one launch: the ncu figure per cell-update (profiles/) x
+    # the cell-updates of one launch (2D: one pass of the default depth 6 on
+    # grids >= 2^20 cells; 3D: one step of every member)
+    traffic = None
+    tfile = ROOT / "profiles" / f"{kname}_traffic.txt"
+    per_launch = cells * (6 if kname == "k2d_pass" and cells >= 1 << 20 else 1)
+    if tfile.exists() and (kname != "k2d_pass" or args.tune is None):
+        for tl in tfile.read_text().splitlines():
+            if tl.startswith("dram_bytes_per_cell_update="):
+                traffic = float(tl.split("=")[1]) * per_launch
     roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
             "bytes_per_cell_update": bpc,
             "note": f"algorithmic bytes = {bpc} B x cell-updates / run time (all passes); "
                     "temporal blocking re-uses tiles on chip, so frac may exceed 1"}
