@@ -139,3 +139,17 @@ def test_balanced_dataset_writes_samples_and_manifest(cuda, tmp_path):
     for p, label in zip(man["sample_paths"], man["labels"]):
         z = np.load(p, allow_pickle=True)
         assert int(z["label"]) == label and z["signals_total"].shape == (4, 4, 60)
+
+
+@pytest.mark.gpu
+def test_samples_batched_together_equal_reference(cuda, tmp_path):
+    """Two samples (a bleed and a healthy head) advanced in one batched
+    solve give each sample's reference signals bit for bit."""
+    gen = _gen(tmp_path)
+    out = gen.generate_samples([(int(G["nb_label"]), int(G["nb_seed"])),
+                                (int(G["nb0_label"]), int(G["nb0_seed"]))])
+    for tag, smp in zip(("nb", "nb0"), out):
+        assert smp is not None
+        assert _sha(smp["signals_total"]) == str(G[f"{tag}_sha_total"])
+        assert _sha(smp["signals_reference"]) == str(G[f"{tag}_sha_reference"])
+        assert np.array_equal(smp["signals_scattered"], G[f"{tag}_signals_scattered"])

@@ -161,14 +161,10 @@ class BrainDatasetGenerator:
         return sig[:n].copy(), sig[n:].copy(), mc
 
     # ------------------------------------------------------------------
-    def generate_sample(self, label: int, seed: int, phantom_id: str = "train",
-                        bleed_age: Optional[str] = None,
-                        bleed_size: Optional[str] = None) -> Optional[dict]:
-        """One sample with its own head geometry (generator.py:254-416).
-        ``label`` 0 healthy, 1 epidural, 2 subdural, 3 intracerebral; test
-        samples draw geometry from seed + 10^7.  For a bleed, up to 50
-        (geometry seed, size) combinations are tried, sizes falling back to
-        smaller ones; None when none fits."""
+    def _prepare(self, label: int, seed: int, phantom_id: str, bleed_age: Optional[str],
+                 bleed_size: Optional[str]):
+        """Head geometry, bleed and the two phantoms of one sample
+        (generator.py:254-336), or None when no bleed placement fits."""
         rng = random.Random(seed)
         geom_seed = seed if phantom_id == "train" else seed + 10_000_000
         geom = sample_random_geometry(seed=geom_seed, grid_size=self._N, dx_mm=self._dx * 1e3)
@@ -192,13 +188,15 @@ class BrainDatasetGenerator:
             if bleed is None:
                 return None
         reference = BrainPhantom3D(self._grid, self._freq_hz, geometry=geom, seed=seed + 100000)
+        return geom, bleed, target, reference
 
-        signals_total, signals_ref, mc = self._run_pair(target, reference)
+    def _finish(self, label, seed, phantom_id, geom, bleed, signals_total, signals_ref, mc):
+        """Scattered signals, layered DAS image and the sample dict
+        (generator.py:340-416)."""
         signals_scattered = signals_total - signals_ref
         head_geom = {"cx_cells": geom.center[0], "cy_cells": geom.center[1],
                      "layers": [(getattr(geom, f), e) for f, e in _DAS_LAYER_EPS]}
         das_image = self._ring.compute_das_image(signals_scattered, head_geometry=head_geom)
-
         center = bleed.center if bleed else (0, 0, 0)
         r = bleed.radius if bleed else 0
         r_mm = r * self._dx * 1e3
@@ -234,6 +232,47 @@ class BrainDatasetGenerator:
             "_mcells_per_second": np.float32(mc),
         }
 
+    def generate_sample(self, label: int, seed: int, phantom_id: str = "train",
+                        bleed_age: Optional[str] = None,
+                        bleed_size: Optional[str] = None) -> Optional[dict]:
+        """One sample with its own head geometry (generator.py:254-416).
+        ``label`` 0 healthy, 1 epidural, 2 subdural, 3 intracerebral; test
+        samples draw geometry from seed + 10^7.  For a bleed, up to 50
+        (geometry seed, size) combinations are tried, sizes falling back to
+        smaller ones; None when none fits."""
+        return self.generate_samples([(label, seed)], phantom_id, bleed_age, bleed_size)[0]
+
+    def generate_samples(self, specs, phantom_id: str = "train", bleed_age: Optional[str] = None,
+                         bleed_size: Optional[str] = None) -> list:
+        """Several samples, ``specs`` = [(label, seed), ...], with every
+        acquisition of all of them (2 x n_tx solves per sample) advanced in
+        one batched solve; each sample equals ``generate_sample`` of its spec
+        (None where the bleed does not fit)."""
+        prep = [self._prepare(label, seed, phantom_id, bleed_age, bleed_size)
+                for label, seed in specs]
+        live = [p for p in prep if p is not None]
+        out = [None] * len(specs)
+        if not live:
+            return out
+        n = self._n_tx
+        coeffs, tx = [], []
+        for _, _, target, reference in live:
+            ct, cr = target.build_device(self._device), reference.build_device(self._device)
+            coeffs += [ct] * n + [cr] * n
+            tx += list(range(n)) * 2
+        traces, mc = self._run_members(coeffs, tx)
+        sig = traces.cpu().numpy()
+        q = 0
+        for k, p in enumerate(prep):
+            if p is None:
+                continue
+            geom, bleed, _, _ = p
+            total = sig[2 * n * q:2 * n * q + n].copy()
+            ref = sig[2 * n * q + n:2 * n * (q + 1)].copy()
+            out[k] = self._finish(specs[k][0], specs[k][1], phantom_id, geom, bleed, total, ref, mc)
+            q += 1
+        return out
+
     def save_sample_async(self, sample: dict, sample_idx: int) -> Future:
         """``save_sample`` on a background writer thread (zlib compression
         releases the GIL, so the next sample's solve overlaps the write);
@@ -262,11 +301,14 @@ class BrainDatasetGenerator:
         return path
 
     def generate_balanced_dataset(self, n_samples: int, phantom_id: str = "train",
-                                  base_seed: int = 0, show_progress: bool = True) -> dict:
+                                  base_seed: int = 0, show_progress: bool = True,
+                                  batch_samples: int = 4) -> dict:
         """``n_samples`` split evenly over the four classes in a seeded
         shuffled order; sample i of class c uses seed base + 7 i + 1000 c;
         samples whose bleed does not fit are skipped and counted.  Writes
-        ``manifest.json`` and returns it (generator.py:434-539)."""
+        ``manifest.json`` and returns it (generator.py:434-539).  New:
+        ``batch_samples`` consecutive samples share one batched solve (their
+        results are the same as one at a time)."""
         per = n_samples // 4
         labels = [0] * per + [1] * per + [2] * per + [3] * per
         labels += [i % 4 for i in range(n_samples - len(labels))]
@@ -280,31 +322,43 @@ class BrainDatasetGenerator:
         }
         t_start = time.time()
         idx = 0
-        for i, label in enumerate(labels):
-            sample = self.generate_sample(label=label, seed=base_seed + i * 7 + label * 1000,
-                                          phantom_id=phantom_id)
-            if sample is None:
-                manifest["n_failed"] += 1
-                if show_progress:
-                    print(f"  [{i + 1}/{n_samples}] SKIP (bleed placement failed, label={label})")
-                continue
-            path = self._output_dir / f"sample_{idx:06d}.npz"
-            self.save_sample_async(sample, idx)
-            manifest["n_completed"] += 1
-            manifest["class_counts"][int(label)] += 1
-            manifest["sample_paths"].append(str(path))
-            manifest["sample_indices"].append(idx)
-            manifest["labels"].append(int(label))
-            manifest["bleed_types"].append(str(sample["bleed_type"]))
-            manifest["bleed_ages"].append(str(sample["bleed_age"]))
-            if show_progress:
-                el = time.time() - t_start
-                eta = el / (i + 1) * (n_samples - i - 1)
-                print(f"  [{i + 1:4d}/{n_samples}] label={label} type={sample['bleed_type']:15} "
-                      f"age={sample['bleed_age']:9} {float(sample['_mcells_per_second']):.1f}Mc/s "
-                      f"ETA:{eta / 60:.0f}min")
-            idx += 1
+        group = max(1, int(batch_samples))
+        for i0 in range(0, len(labels), group):
+            part = list(enumerate(labels[i0:i0 + group], start=i0))
+            specs = [(label, base_seed + i * 7 + label * 1000) for i, label in part]
+            for (i, label), sample in zip(part, self.generate_samples(specs, phantom_id=phantom_id)):
+                idx = self._record(manifest, i, label, sample, idx, n_samples, t_start,
+                                   show_progress)
         self.flush()
+        return self._write_manifest(manifest, n_samples, show_progress)
+
+    def _record(self, manifest: dict, i: int, label: int, sample: Optional[dict], idx: int,
+                n_samples: int, t_start: float, show_progress: bool) -> int:
+        """Manifest entry and background write of one sample; returns the
+        next sample index."""
+        if sample is None:
+            manifest["n_failed"] += 1
+            if show_progress:
+                print(f"  [{i + 1}/{n_samples}] SKIP (bleed placement failed, label={label})")
+            return idx
+        path = self._output_dir / f"sample_{idx:06d}.npz"
+        self.save_sample_async(sample, idx)
+        manifest["n_completed"] += 1
+        manifest["class_counts"][int(label)] += 1
+        manifest["sample_paths"].append(str(path))
+        manifest["sample_indices"].append(idx)
+        manifest["labels"].append(int(label))
+        manifest["bleed_types"].append(str(sample["bleed_type"]))
+        manifest["bleed_ages"].append(str(sample["bleed_age"]))
+        if show_progress:
+            el = time.time() - t_start
+            eta = el / (i + 1) * (n_samples - i - 1)
+            print(f"  [{i + 1:4d}/{n_samples}] label={label} type={sample['bleed_type']:15} "
+                  f"age={sample['bleed_age']:9} {float(sample['_mcells_per_second']):.1f}Mc/s "
+                  f"ETA:{eta / 60:.0f}min")
+        return idx + 1
+
+    def _write_manifest(self, manifest: dict, n_samples: int, show_progress: bool) -> dict:
         path = self._output_dir / "manifest.json"
         with open(path, "w") as fh:
             json.dump(manifest, fh, indent=2)
