@@ -122,7 +122,9 @@ def test_streaming_kernel_equals_tile_kernel_multi_block(cuda, mat, tma_shape):
     srcs = []
     for c, (i, j, k) in (("Ez", (11, 14, 30)), ("Hy", (5, 15, 31)), ("Ex", (0, 0, 0)),
                          ("Hx", (22, 36, nz - 1)), ("Ey", (12, 28, 59)), ("Ez", (20, 13, 29)),
-                         ("Ex", (3, 27, 60))):
+                         ("Ex", (3, 27, 60)),
+                         # E sources on the extra box row of the TMA blocks (15 core rows)
+                         ("Ex", (7, 15, 20)), ("Ez", (9, 30, 44)), ("Ey", (13, 30, 2))):
         srcs.append((c, (i, i + 1, j, j + 1, k, k + 1),
                      torch.from_numpy(rng.standard_normal(steps).astype(np.float32))))
     ca = cb = None

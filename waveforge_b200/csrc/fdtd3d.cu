@@ -761,7 +761,7 @@ static TmaEncodeFn tma_encoder() {
   return fn;
 }
 
-// 4D map {k, j, i, instance} of one float32 array with a kBoxK x kTJ x 1 x 1
+// 4D map {k, j, i, instance} of one float32 array with a kBoxK x kBoxJ x 1 x 1
 // box; false when the layout breaks a TMA rule (16-byte strides / base).
 static bool tma_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, int ninst,
                     long long istride) {
@@ -773,7 +773,7 @@ static bool tma_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, i
   const long long plane = (long long)nx * ny * nz;
   const cuuint64_t strides[3] = {(cuuint64_t)nz * 4, (cuuint64_t)ny * nz * 4,
                                  (cuuint64_t)(ninst > 1 ? istride : plane) * 4};
-  const cuuint32_t box[4] = {(cuuint32_t)kBoxK, (cuuint32_t)kTJ, 1, 1};
+  const cuuint32_t box[4] = {(cuuint32_t)kBoxK, (cuuint32_t)kBoxJ, 1, 1};
   const cuuint32_t es[4] = {1, 1, 1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(base), dims, strides, box,
             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

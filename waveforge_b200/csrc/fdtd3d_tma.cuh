@@ -25,10 +25,15 @@
 
 namespace wf {
 
-constexpr int kTJ = 16, kTK = 32, kTCJ = kTJ - 2, kTCK = kTK - 2;
+// 16 thread rows (j) x 32 lanes (k); row 0 and lanes 0, 31 are halo.  The box
+// holds one more row (16) than the threads: the E of row 16 completes the curl
+// of row 15, which makes rows 1..15 core (15 per block instead of 14).
+constexpr int kTJ = 16, kTK = 32, kTCJ = kTJ - 1, kTCK = kTK - 2;
+constexpr int kBoxJ = kTJ + 1;                  // box height in j
 constexpr int kBoxK = 36;                       // box width in k (>= 32 + 3 + 1)
 constexpr int kRing = 4;                        // i-plane slots
-constexpr int kTileF = kTJ * kBoxK;             // floats per array per slot
+constexpr int kBoxF = kBoxJ * kBoxK;            // floats one box load writes
+constexpr int kTileF = (kBoxF + 31) / 32 * 32;  // floats per array per slot (128-byte aligned)
 constexpr int kSlotF = 8 * kTileF;              // floats per slot
 constexpr int kHcF = kTJ * kTK;                 // floats per H row set component
 constexpr int kHcSetF = 3 * kHcF;               // floats per plane of hc
@@ -39,7 +44,7 @@ struct TmaMaps {
 };
 
 struct TmaSmem {
-  float raw[kRing][8][kTJ][kBoxK];  // slot, array, row, column
+  float raw[kRing][8][kTileF];      // slot, array, row * kBoxK + column
   float hc[3][3][kTJ][kTK];         // curl-updated H of planes (p mod 3)
   float hf[3][kTJ][kTK];            // final H of plane f
   float hom[2][kTJ][kTK];           // old Hy, Hz of plane Nx-2 (x face at Nx-1)
@@ -121,7 +126,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy),
                rdz = __drcp_rn((double)dz);
   const int narr = MAT ? 8 : 6;
-  const unsigned bytes = (unsigned)(narr * kTileF * sizeof(float));
+  const unsigned bytes = (unsigned)(narr * kBoxF * sizeof(float));  // what the loads deliver
 
   if (tid == 0) {
     for (int s = 0; s < kRing; ++s) mbar_init(&S.bar[s], 1);
@@ -129,7 +134,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     int nh = 0, ne = 0;
     for (int q = 0; q < P.nsrc; ++q) {
       const wf_source& Q = P.src[q];
-      if (Q.i1 <= f0 || Q.i0 > plast || Q.j1 <= j0 || Q.j0 >= j0 + kTJ || Q.k1 <= k0 ||
+      if (Q.i1 <= f0 || Q.i0 > plast || Q.j1 <= j0 || Q.j0 >= j0 + kBoxJ || Q.k1 <= k0 ||
           Q.k0 >= k0 + kTK)
         continue;
       if (Q.comp >= WF_HX) {
@@ -160,16 +165,17 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     // before the asynchronous-proxy overwrite
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&S.bar[s], bytes);
-    for (int c = 0; c < 6; ++c) tma_load4(&S.raw[s][c][0][0], &maps.m[c], kb, j0, p, inst, &S.bar[s]);
+    for (int c = 0; c < 6; ++c) tma_load4(&S.raw[s][c][0], &maps.m[c], kb, j0, p, inst, &S.bar[s]);
     if (MAT) {
-      tma_load4(&S.raw[s][6][0][0], &maps.m[6], kb, j0, p, ci_inst, &S.bar[s]);
-      tma_load4(&S.raw[s][7][0][0], &maps.m[7], kb, j0, p, ci_inst, &S.bar[s]);
+      tma_load4(&S.raw[s][6][0], &maps.m[6], kb, j0, p, ci_inst, &S.bar[s]);
+      tma_load4(&S.raw[s][7][0], &maps.m[7], kb, j0, p, ci_inst, &S.bar[s]);
     }
   };
   unsigned phase = 0u;  // parity bit per slot
   bool failed = false;
-  // Wait for plane p, then add this CTA's E-source values into it (each
-  // column-owner adds to its own cell).
+  // Wait for plane p, then add this CTA's E-source values into it: each
+  // thread to its own cell, the last thread row also to the box's extra row.
+  const bool in16 = w == kTJ - 1 && gj + 1 < ny && gk >= 0 && gk < nz;
   auto land = [&](int p) {
     const int s = p % kRing;
     const unsigned par = (phase >> s) & 1u;
@@ -181,13 +187,17 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       }
     }
     phase ^= 1u << s;
-    if (ne > 0 && in) {
+    if (ne > 0 && (in || in16)) {
       for (int q = 0; q < ne; ++q) {
         const wf_source& Q = P.src[S.L.e[q]];
-        if (p >= Q.i0 && p < Q.i1 && gj >= Q.j0 && gj < Q.j1 && gk >= Q.k0 && gk < Q.k1) {
-          const float v = src3_value(Q, p, gj, gk, n);
-          float& cell = S.raw[s][Q.comp][w][col];
-          cell = fadd(cell, v);
+        if (p < Q.i0 || p >= Q.i1 || gk < Q.k0 || gk >= Q.k1) continue;
+        if (in && gj >= Q.j0 && gj < Q.j1) {
+          float& cell = S.raw[s][Q.comp][w * kBoxK + col];
+          cell = fadd(cell, src3_value(Q, p, gj, gk, n));
+        }
+        if (in16 && gj + 1 >= Q.j0 && gj + 1 < Q.j1) {
+          float& cell = S.raw[s][Q.comp][kTJ * kBoxK + col];
+          cell = fadd(cell, src3_value(Q, p, gj + 1, gk, n));
         }
       }
     }
@@ -195,7 +205,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
 
   // Per-thread shared-memory bases: slot arrays are addressed as
   // R[c * kTileF] (+ kBoxK for j + 1, + 1 for k + 1), H rows as Hrow[c * kHcF].
-  float* const raw0 = &S.raw[0][0][0][0] + (w * kBoxK + col);
+  float* const raw0 = &S.raw[0][0][0] + (w * kBoxK + col);
   float* const hc0 = &S.hc[0][0][0][0] + (w * kTK + lane);
   const bool cjk = gj < ny - 1 && gk < nz - 1, ck = gk < nz - 1, cj = gj < ny - 1;
   // a block none of whose cells lies on a j or k face needs the Mur code only
@@ -290,7 +300,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     float hxF = hcur.x, hyF = hcur.y, hzF = hcur.z;
     if (p < nx) curl(p, false);
     const int sf = f & (kRing - 1), hf0 = f % 3;
-    auto Ho = [&](int c, int ww, int ll) -> float { return S.raw[sf][3 + c][ww][ll + cofs]; };
+    auto Ho = [&](int c, int ww, int ll) -> float { return S.raw[sf][3 + c][ww * kBoxK + ll + cofs]; };
     if (f == nx - 2) {
       S.hom[0][w][lane] = Ho(1, w, lane);
       S.hom[1][w][lane] = Ho(2, w, lane);
@@ -303,7 +313,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       auto Hc = [&](int c, int ww, int ll) -> float { return S.hc[hf0][c][ww][ll]; };
       // Hy, Hz after the x faces
       auto xf = [&](int c, int ww, int ll) -> float {
-        if (f == 0) return fadd(S.raw[sp][3 + c][ww][ll + cofs],
+        if (f == 0) return fadd(S.raw[sp][3 + c][ww * kBoxK + ll + cofs],
                                 fmul(mx, fsub(S.hc[hp][c][ww][ll], Ho(c, ww, ll))));
         if (f == nx - 1) return fadd(S.hom[c - 1][ww][ll], fmul(mx, fsub(S.hc[hm][c][ww][ll], Ho(c, ww, ll))));
         return Hc(c, ww, ll);
