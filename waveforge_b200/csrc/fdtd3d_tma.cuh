@@ -2,12 +2,14 @@
 // i-planes staged in shared memory by the Tensor Memory Accelerator.
 // Included by fdtd3d.cu (uses Tile3D, Lists3D, dv<>, src3_value).
 //
-// A CTA owns a 16 (j) x 32 (k) block of columns -- a 14 x 30 core with a
-// one-cell halo -- and walks an i-segment exactly like k3d_stream, with the
-// same float ops in the same order (so the two are bit-identical).  What
-// changes is data movement: one thread issues, per i-plane, one
-// cp.async.bulk.tensor load per array (Ex, Ey, Ez, Hx, Hy, Hz and Ca, Cb) of a
-// 16 x 36 box into a 4-slot shared-memory ring, completing on the slot's
+// A CTA of 16 (j) x 32 (k) threads owns a block of columns -- a 15 x 30 core
+// behind a one-cell halo at j - 1, k - 1 and k + 1 -- and walks an i-segment
+// exactly like k3d_stream, with the same float ops in the same order (so the
+// two are bit-identical).  What changes is data movement: one thread issues,
+// per i-plane, one cp.async.bulk.tensor load per array (Ex, Ey, Ez, Hx, Hy, Hz
+// and Ca, Cb) of a 17 x 36 box (one j-row more than the threads: the E of the
+// last thread row's j + 1 neighbours) into a 4-slot shared-memory ring,
+// completing on the slot's
 // mbarrier.  A thread keeps E, Ca and Cb of its cell of plane f in registers
 // from the Faraday step of that plane, so plane f's slot is refilled with
 // plane f + 4 as soon as the plane-f step starts (after the Mur code on face
