@@ -393,6 +393,75 @@ def cpu_single_sample(make_oracle, cells, max_steps, budget_s=12.0):
             f"({cells * done:.3e} cell-updates in {t:.1f} s)")
 
 
+def companion_legs(args, dev):
+    """The rest of the metric on the same GPU, reported beside the headline:
+    the plain kernel at 4096^2 (its HBM-roofline target), the 256^3 head
+    solve, and the served stream with p50/p99 latency.  Each runs its whole
+    workload once untimed, then is timed with CUDA events (plain2d, head3d:
+    two full solves; serve: one full stream and its one-at-a-time baseline)."""
+    import copy
+    from waveforge_b200 import workloads as W
+    from waveforge_b200.serving import Server, serve_one_at_a_time
+    peak, peak_kind = measured_peaks()
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for wk, nsteps, side in (("plain2d", 2000, 4096), ("head3d", 1500, 256)):
+        a = copy.copy(args)
+        a.workload, a.nsteps, a.side, a.tune, a.instances = wk, nsteps, side, None, 1
+        sim, det, _, _, _, cells, bpc, _, name, kname = build_single(a, dev)
+        sim.reset()
+        sim.run(nsteps, record=det)
+        ms = []
+        for _ in range(2):
+            sim.reset()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.run(nsteps, record=det)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms.append(e0.elapsed_time(e1))
+        t = statistics.mean(ms) * 1e-3
+        gcu = cells * nsteps / t / 1e9
+        dram = None
+        tfile = ROOT / "profiles" / f"{kname}_traffic.txt"
+        if tfile.exists():
+            for tl in tfile.read_text().splitlines():
+                if tl.startswith("dram_bytes_per_cell_update="):
+                    dram = float(tl.split("=")[1])
+        out[f"{wk}_{side}"] = {
+            "workload": name, "value": gcu, "unit": UNIT, "ms_per_solve": t * 1e3,
+            "kernel": kname, "bytes_per_cell_update": bpc,
+            "frac_algorithmic": gcu * bpc / peak, "peak_gbs": peak, "peak_kind": peak_kind,
+            "dram_bytes_per_cell_update_ncu": dram,
+            "dram_frac_of_peak": None if dram is None else gcu * dram / peak}
+        del sim, det
+        torch.cuda.empty_cache()
+    arrivals = W.ServingStream(rate=200.0, duration=10.0, seed=args.seed,
+                               grad_fraction=0.1).arrivals()
+    warm = W.ServingStream(rate=20.0, duration=0.3, seed=args.seed + 1, side_max=256,
+                           steps_max=1200).arrivals()
+    Server(dev, max_wait_s=2.0).serve(warm)
+    srv = Server(dev, chunk_steps=128, max_wait_s=2.0, hbm_budget=60e9, max_active_cells=3.2e7)
+    tickets = srv.serve(arrivals)
+    stats = _stream_stats(tickets, max(t.t_done for t in tickets if t.t_done is not None))
+    base = serve_one_at_a_time(dev, arrivals, max_wait_s=2.0)
+    bstats = _stream_stats(base, max(t.t_done for t in base if t.t_done is not None))
+    out["serve"] = {
+        "workload": "serve_poisson200_10s_side128-1024_steps1000-5000_16tx_grad10pct",
+        "requests": len(arrivals), "p50_s": stats["p50_s"], "p99_s": stats["p99_s"],
+        "served": stats["served"], "rejected": stats["rejected"],
+        "gradient_served": stats["gradient_served"],
+        "served_gcell_upd_per_s": stats["gcell_upd_per_s"], "solves_per_s": stats["solves_per_s"],
+        "one_at_a_time": {"p50_s": bstats["p50_s"], "p99_s": bstats["p99_s"],
+                          "served": bstats["served"], "rejected": bstats["rejected"],
+                          "served_gcell_upd_per_s": bstats["gcell_upd_per_s"]},
+        "policy": "FIFO admission by HBM footprint (60 GB) and in-flight cells; reject at "
+                  "arrival when the estimated wait exceeds 2 s; latency = arrival -> traces "
+                  "(and gradients) in pinned host memory"}
+    return out
+
+
 def bench_single(args, ws, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -794,6 +863,8 @@ def main():
                     help="dataset: samples whose acquisitions share one batched solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="mimo: skip the plain2d/head3d/serve companion legs")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -916,19 +987,21 @@ def main():
             host_traces[t].copy_(batches[t]._traces, non_blocking=True)
         host_images.copy_(images, non_blocking=True)
 
-    for _ in range(args.warmup):
+    # the e2e leg repeats the same multi-second step: a few steps bound it tightly
+    e2e_steps = min(args.steps, 5)
+    for _ in range(min(args.warmup, 3)):
         e2e_step()
     torch.cuda.synchronize(dev)
     barrier(ws)
     s2 = torch.cuda.Event(enable_timing=True)
     e2 = torch.cuda.Event(enable_timing=True)
     s2.record(stream)
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         e2e_step()
     e2.record(stream)
     torch.cuda.synchronize(dev)
     barrier(ws)
-    ms_e2e = reduce_max(s2.elapsed_time(e2), ws, dev) / args.steps
+    ms_e2e = reduce_max(s2.elapsed_time(e2), ws, dev) / e2e_steps
     e2e_value = ws * cells_per_step / (ms_e2e * 1e-3) / 1e9
 
     # ---- plain per-solve comparison (stratified sample) -------------------
@@ -986,6 +1059,10 @@ def main():
                                        "(persistent: one launch; tiled: all its pass launches); "
                                        "temporal blocking re-uses tiles on chip, so frac may exceed 1"}
 
+    extra = {}
+    if ws == 1 and not args.no_extras:
+        extra = companion_legs(args, dev)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         v, cores, sample = cpu_reference_sample()
@@ -1006,10 +1083,14 @@ def main():
                        [batches[True].depth, *batches[True].region, batches[True].threads],
                        "parallelism": f"replicas x{ws}"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e, "steps": e2e_steps},
             "plain_per_solve": plain, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": args.steps * (2 * batches[True].launches_per_run() + len(phantoms)),
         }
+        if "serve" in extra:
+            line["latency_s"] = {"p50": extra["serve"]["p50_s"], "p99": extra["serve"]["p99_s"],
+                                 "of": "the served Poisson stream (key serve)"}
+        line.update(extra)
         print(json.dumps(line), flush=True)
     barrier(ws)
 

@@ -54,8 +54,9 @@ typedef struct wf_grid2d {
   int32_t flags; /* WF_FASTDIV_* bits: set only after wf_check_fastdiv passed */
 } wf_grid2d;
 
-/* wf_grid*.flags: divisions by this spacing may use the FMA-corrected
- * reciprocal, which wf_check_fastdiv proved identical to IEEE division for
+/* wf_grid*.flags: divisions by this spacing may be computed as
+ * float32(double(x) * double(1/d)) -- one float64 product rounded once to
+ * float32 -- which wf_check_fastdiv proved identical to IEEE division for
  * every float32 input.  Without the bit the kernels use IEEE division. */
 #define WF_FASTDIV_X 1
 #define WF_FASTDIV_Y 2
@@ -153,9 +154,11 @@ int32_t wf_fdtd2d_run(const wf_grid2d* g,
  * the library until the process exits); grids above WF_NOALLOC_MAX_CELLS
  * cells are rejected with WF_E_LIMIT.  Nothing is allocated.  The first call
  * on each device looks the array's device address up once, so make that
- * first call before any stream capture.  All calls on a device share the
- * array: calls that may overlap on the GPU race and must be serialised by
- * the caller.  Nothing in the array needs to start at zero. */
+ * first call before any stream capture; the address is cached for the
+ * device's CUDA context, so after cudaDeviceReset reload the library before
+ * the next call.  All calls on a device share the array: calls that may
+ * overlap on the GPU race and must be serialised by the caller.  Nothing in
+ * the array needs to start at zero.  Negative sizes give WF_E_ARG. */
 #define WF_NOALLOC_MAX_CELLS (1LL << 20)
 int32_t wf_fdtd2d_run_noalloc(const wf_grid2d* g,
                               float* ex, float* ey, float* hz,
@@ -353,6 +356,16 @@ int32_t wf_cpml2d_run(const wf_grid2d* g, float* ex, float* ey, float* hz, const
                       int32_t nprobe, float* traces, int64_t trace_ld, int32_t trace_step0,
                       int32_t step0, int32_t nsteps, int32_t n_check, uint32_t* check_max,
                       void* stream);
+
+/* Bound of the TMA pass's shared-memory pipeline waits, for every later 3D
+ * launch of this process: each wait takes one non-blocking look, then at
+ * most `polls` hardware-suspended polls before it gives up with WF_E_TIMEOUT
+ * (see wf_fdtd3d_take_status).  polls < 0 restores the built-in bound
+ * (2^22).  A small bound makes the pass give up on loads that do complete:
+ * failure-handling tests use it to take the timeout path without any device
+ * fault.  The wait for copies still in flight after a give-up always uses
+ * the built-in bound.  No reference counterpart. */
+int32_t wf_fdtd3d_set_wait_limit(int64_t polls);
 
 /* Status of the 3D passes since the last call on this device, then cleared:
  * 0, or WF_E_TIMEOUT when a bounded shared-memory pipeline wait of the TMA

@@ -1,7 +1,7 @@
 """Generate the golden vectors of the parity tests by running the REFERENCE.
 
 Run in a container that holds the read-only reference checkout:
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref /root/reference [--only case,...]
 
 It imports the reference's own ``core`` package and example DAS functions
 (pure Python + PyTorch, CPU), runs each case in float32 and float64, and
@@ -81,10 +81,13 @@ def gauss_deriv_class(R):
 
 
 def run_2d(R, nx, ny, dx, courant, steps, dtype, paint=None, default=None, sources=(), probes=(),
-           n_check=10 ** 9):
-    """sources: (comp, kind, args, wave_tensor) ; probes: (comp, i, j)."""
+           n_check=10 ** 9, init=None):
+    """sources: (comp, kind, args, wave_tensor) ; probes: (comp, i, j);
+    init: {component: float32 (nx, ny) array} of starting values."""
     grid = R["grid"].YeeGrid(nx, ny, dx, dx, courant=courant, device="cpu", dtype=dtype)
     f = R["fields"].FieldSet(grid)
+    for c, v in (init or {}).items():
+        getattr(f, c).copy_(torch.from_numpy(v).to(dtype).reshape(getattr(f, c).shape))
     b = R["boundaries"].MurABC(grid, f.Hz)
     Ca = Cb = None
     if paint is not None:
@@ -184,8 +187,9 @@ def case_lossy_ellipses(R, out, n=256, steps=600):
         hz64_dec=dec(f64.Hz[::4, :, 0].numpy(), 4))
 
 
-def case_breast_mimo(R, out, sides=(150, 200), n_tx=2, steps=1500):
-    """Two breast phantoms (fixed sides), first n_tx transmitters each, 16 receivers."""
+def case_breast_mimo(R, out, sides=(150, 200), n_tx=2, steps=1500, name="breast_mimo_small"):
+    """Breast phantoms of the given sides (drawn in order from the workload's
+    seed), first n_tx transmitters each, 16 receivers."""
     wl = W.BreastMIMO(n_phantoms=len(sides), steps=steps)
     rng = np.random.default_rng(wl.seed)
     phantoms = [W.BreastPhantom.draw(rng, side=s) for s in sides]
@@ -220,7 +224,7 @@ def case_breast_mimo(R, out, sides=(150, 200), n_tx=2, steps=1500):
             data[key + "_traces64_dec"] = dec(tr64.numpy(), 5)
             data[f"p{p_idx}_sha_ca"] = sha(ca)
             data[f"p{p_idx}_sha_cb"] = sha(cb)
-    np.savez_compressed(out / "breast_mimo_small.npz", **data)
+    np.savez_compressed(out / f"{name}.npz", **data)
 
 
 def case_edges_2d(R, out):
@@ -294,10 +298,16 @@ def case_edges_2d(R, out):
         np.savez_compressed(out / f"edges2d_{name}.npz", **d)
 
 
-def run_3d(R, shape, dx, courant, steps, dtype, paint=None, default=None, sources=(), probes=()):
+def run_3d(R, shape, dx, courant, steps, dtype, paint=None, default=None, sources=(), probes=(),
+           init=None, batch=1):
+    """probes: (comp, i, j, k), recorded for every batch member (rows
+    member-major when batch > 1); init: {component: float32 array of the
+    field shape, (batch, nx, ny, nz) when batched}."""
     nx, ny, nz = shape
     grid = R["grid"].YeeGrid(nx, ny, dx, dx, Nz=nz, dz=dx, courant=courant, device="cpu", dtype=dtype)
-    f = R["fields"].FieldSet(grid)
+    f = R["fields"].FieldSet(grid, batch_size=batch)
+    for c, v in (init or {}).items():
+        getattr(f, c).copy_(torch.from_numpy(v).to(dtype).reshape(getattr(f, c).shape))
     b = R["boundaries"].MurABC3D(grid, f.Hx, f.Hy, f.Hz)
     Ca = Cb = None
     if paint is not None:
@@ -316,12 +326,15 @@ def run_3d(R, shape, dx, courant, steps, dtype, paint=None, default=None, source
             srcs.append(R["sources"].PlaneSource(w, plane, pos, comp, grid=grid, N_steps=steps))
     sc = R["sources"].SourceCollection(srcs) if srcs else None
     sim = R["fdtd3d"].FDTD3D(grid, f, b, sc, Ca=Ca, Cb=Cb, n_check=10 ** 9)
-    tr = torch.zeros(len(probes), steps, dtype=dtype)
+    if batch == 1:
+        tr = torch.zeros(len(probes), steps, dtype=dtype)
+    else:
+        tr = torch.zeros(batch, len(probes), steps, dtype=dtype)
     with torch.no_grad():
         for s in range(steps):
             sim.step()
             for r, (comp, i, j, k) in enumerate(probes):
-                tr[r, s] = getattr(f, comp)[i, j, k]
+                tr[..., r, s] = getattr(f, comp)[..., i, j, k]
     return grid, f, tr, Ca, Cb
 
 
@@ -505,9 +518,83 @@ def case_brain_dataset(R, ref: Path, out):
     np.savez_compressed(out / "brain_dataset40.npz", **res)
 
 
+def case_lossy_full(R, out, n=4096, steps=100, init_seed=41):
+    """The 4096^2 lossy-ellipse scene at its full size, from seeded random
+    starting fields (so the short run reaches every cell, edge and tile
+    boundary), the ring receivers plus 8 near the source, float32 and
+    float64."""
+    wl = W.LossyEllipses(n=n, steps=steps)
+    GD = gauss_deriv_class(R)
+    M = R["materials"].Material
+    si, sj = wl.source
+    rx = [("Hz", i, j) for i, j in wl.receivers] + [
+        (c, si + di, sj + dj) for c, di, dj in (("Hz", 12, 0), ("Hz", 0, -17), ("Ex", -9, 9),
+                                                ("Ey", 20, 20), ("Hz", 0, 0), ("Ex", 3, -30),
+                                                ("Ey", -25, 4), ("Hz", -30, -30))]
+    init = W.initial_fields(init_seed, (n, n), ("Ex", "Ey", "Hz"))
+    res = {}
+    for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+        grid = R["grid"].YeeGrid(n, n, wl.dx, wl.dx, courant=wl.courant, device="cpu", dtype=dtype)
+        wave = GD().build(steps, grid.dt, torch.device("cpu"), dtype)
+        if dtype == torch.float32:
+            wave32 = wave.clone()
+        res[dt_name] = run_2d(R, n, n, wl.dx, wl.courant, steps, dtype, paint=wl.paint,
+                              default=wl.background(M),
+                              sources=[("Hz", "point", wl.source, wave)], probes=rx, init=init)
+        print("  lossy", n, dt_name, "done", flush=True)
+    g32, f32, tr32, ca, cb = res["32"]
+    _, f64, tr64, _, _ = res["64"]
+    np.savez_compressed(
+        out / f"lossy_full_{n}.npz", n=n, steps=steps, dx=wl.dx, courant=wl.courant,
+        dt=g32.dt, seed=wl.seed, init_seed=init_seed, src=np.array(wl.source),
+        rx_comp=np.array([r[0] for r in rx]), rx=np.array([r[1:] for r in rx]),
+        wave=wave32.numpy(), sha_ca=sha(ca), sha_cb=sha(cb), traces32=tr32.numpy(),
+        traces64=tr64.numpy(), sha_traces=sha(tr32), sha_ex=sha(f32.Ex), sha_ey=sha(f32.Ey),
+        sha_hz=sha(f32.Hz), hz32_dec=np.ascontiguousarray(f32.Hz[::37, ::41, 0].numpy()),
+        hz64_dec=np.ascontiguousarray(f64.Hz[::37, ::41, 0].numpy()))
+
+
+def case_head3d_full(R, out, n=256, steps=30, init_seed=43, batch=1):
+    """The head phantom at a full benchmark size (256^3, or batch x 128^3)
+    from seeded random starting fields of all six components, Ez source at
+    the centre, the ring receivers plus 8 near the source, float32 only
+    (plus float64 traces for the error statement)."""
+    wl = W.Head3D(n=n, steps=steps)
+    GD = gauss_deriv_class(R)
+    M = R["materials"].Material
+    si, sj, sk = wl.source
+    rx = [("Ez", *p) for p in wl.receivers()] + [
+        (c, si + di, sj + dj, sk + dk) for c, di, dj, dk in (
+            ("Ez", 0, 0, 0), ("Ex", 5, -3, 2), ("Ey", -4, 6, 0), ("Hx", 2, 2, -7),
+            ("Hy", -6, 0, 5), ("Hz", 3, -5, 3), ("Ez", 9, 9, -9), ("Ez", 0, 0, 1))]
+    shape = (n, n, n) if batch == 1 else (batch, n, n, n)
+    init = W.initial_fields(init_seed, shape, ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"))
+    res = {}
+    for dt_name, dtype in (("32", torch.float32), ("64", torch.float64)):
+        stable = R["grid"].compute_stable_dt(wl.dx, wl.dx, wl.dx, wl.courant)
+        wave = GD().build(steps, stable, torch.device("cpu"), dtype)
+        if dtype == torch.float32:
+            wave32 = wave.clone()
+        res[dt_name] = run_3d(R, (n, n, n), wl.dx, wl.courant, steps, dtype, paint=wl.paint,
+                              default=wl.background(M),
+                              sources=[("Ez", "point", wl.source, wave)], probes=rx, init=init,
+                              batch=batch)
+        print("  head3d", n, batch, dt_name, "done", flush=True)
+    g, f32, tr32, ca, cb = res["32"]
+    _, f64, tr64, _, _ = res["64"]
+    name = f"head3d_full_{n}" if batch == 1 else f"head3d_batch{batch}x{n}"
+    np.savez_compressed(
+        out / f"{name}.npz", n=n, batch=batch, steps=steps, dx=wl.dx, courant=wl.courant,
+        dt=g.dt, seed=wl.seed, init_seed=init_seed, src=np.array(wl.source),
+        rx_comp=np.array([r[0] for r in rx]), rx=np.array([r[1:] for r in rx]),
+        wave=wave32.numpy(), sha_ca=sha(ca), sha_cb=sha(cb), traces32=tr32.numpy(),
+        traces64=tr64.numpy(), sha_traces=sha(tr32),
+        **{f"sha_{c.lower()}": sha(getattr(f32, c)) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference project checkout")
     ap.add_argument("--only", default="")
     a = ap.parse_args()
     ref = Path(a.ref)
@@ -518,6 +605,11 @@ def main():
         "vacuum": lambda: case_vacuum_point(R, out),
         "lossy": lambda: case_lossy_ellipses(R, out),
         "breast": lambda: case_breast_mimo(R, out),
+        "breast_full": lambda: case_breast_mimo(R, out, sides=(256, 384, 512), n_tx=1, steps=3000,
+                                                name="breast_mimo_full"),
+        "lossy_full": lambda: case_lossy_full(R, out),
+        "head3d_full": lambda: case_head3d_full(R, out),
+        "head3d_batch": lambda: case_head3d_full(R, out, n=128, batch=8, init_seed=47),
         "edges2d": lambda: case_edges_2d(R, out),
         "head3d": lambda: case_head3d(R, out),
         "edges3d": lambda: case_edges_3d(R, out),

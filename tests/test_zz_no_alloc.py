@@ -6,9 +6,10 @@ can synchronise the device), so they cannot supply the scratch fields that
 wf_fdtd2d_run needs.  wf_fdtd2d_run_noalloc keeps that scratch in a device
 array built into the library.  This test calls it through the C-ABI, twice in
 a row (the second call starts from whatever the first left in the shared
-array), and demands the same bits as wf_fdtd2d_run with caller scratch, our
-parity tolerance.  It also checks the size limit is enforced.  The file is
-named to be collected last.
+array), after a call on a grid of another shape has left non-zero values at
+other cells of that array, and demands the same bits as wf_fdtd2d_run with
+caller scratch, our parity tolerance.  It also checks the size limit and the
+rejection of negative sizes.  The file is named to be collected last.
 """
 
 from __future__ import annotations
@@ -57,8 +58,22 @@ def _run(lib, dev, noalloc, g, fields, ca, cb, src_d, prb_d, traces, step0, nste
     nat.check(rc)
 
 
+def _plant_leftovers(lib, dev):
+    """Run the no-alloc entry point once on a grid of another shape with
+    non-zero fields, so the shared array holds values that sit at other cells
+    (a different row length) than the calls that follow will use."""
+    nx, ny, steps = 97, 233, 5
+    g, ca, cb, wave, src_d, prb_d = _case(dev, nx, ny, steps, 11)
+    gen = torch.Generator(device="cpu").manual_seed(3)
+    fields = [torch.randn((nx, ny), generator=gen).to(dev) for _ in range(3)]
+    traces = torch.zeros((3, 2 * steps), dtype=torch.float32, device=dev)
+    _run(lib, dev, True, g, fields, ca, cb, src_d, prb_d, traces, 0, steps)
+    torch.cuda.synchronize(dev)
+
+
 def test_noalloc_matches_caller_scratch_on_two_calls(cuda):
     lib = nat.load()
+    _plant_leftovers(lib, cuda)
     nx, ny, steps = 203, 151, 37
     g, ca, cb, wave, src_d, prb_d = _case(cuda, nx, ny, steps, 5)
     out = {}
@@ -92,3 +107,15 @@ def test_noalloc_rejects_grids_above_its_limit(cuda):
                                    1, 0, None, None, nat.stream_handle(cuda))
     assert rc == nat.WF_E_LIMIT
     assert b"limit" in lib.wf_last_error()
+
+
+def test_noalloc_rejects_negative_sizes(cuda):
+    lib = nat.load()
+    dummy = torch.zeros(1, device=cuda)
+    for nx, ny in ((-1, 8), (8, -3)):
+        g = nat.WfGrid2D(nx, ny, 1.0, 1.0, 1.0, 1.0, -0.5, -0.5, 0)
+        rc = lib.wf_fdtd2d_run_noalloc(ctypes.byref(g), dummy.data_ptr(), dummy.data_ptr(),
+                                       dummy.data_ptr(), None, None, None, 0, None, 0, None, 0,
+                                       0, 0, 1, 0, None, None, nat.stream_handle(cuda))
+        assert rc == nat.WF_E_ARG
+        assert b"negative" in lib.wf_last_error()

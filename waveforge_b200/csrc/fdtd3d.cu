@@ -11,6 +11,8 @@
 //   evaluated as pure functions of pre-step and curl-updated H; Ampere
 //   updates of Ex (j,k>=1), Ey (i,k>=1), Ez (i,j>=1); detectors; maxima.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 #include "wf_common.cuh"
 
@@ -783,12 +785,17 @@ static bool tma_map(CUtensorMap* m, const float* base, int nx, int ny, int nz, i
 // Status word of the TMA pass: a bounded mbarrier wait that gives up writes
 // WF_E_TIMEOUT here (and its CTA stops); wf_fdtd3d_take_status reads and
 // clears it.  Host code passes its device address, looked up once per device.
+// The cached address is that of the current CUDA context of the device: it
+// stays valid until cudaDeviceReset, after which this library must be
+// reloaded (the same holds for every cached module address in it).
 static __device__ int g_tma_status;
+static std::mutex g_tma_mu;  // guards the caches below (host threads may race)
 
 static int* tma_status_ptr() {
   static int* ptr[64] = {nullptr};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(g_tma_mu);
   if (ptr[dev] == nullptr) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_tma_status) != cudaSuccess) return nullptr;
@@ -797,16 +804,25 @@ static int* tma_status_ptr() {
   return ptr[dev];
 }
 
-// Opt k3d_tma into its dynamic shared memory (once per instantiation).
+// Suspended polls a TMA pipeline wait makes after its first non-blocking look
+// (negative = kSpinLimit); see wf_fdtd3d_set_wait_limit.
+static std::atomic<long long> g_tma_wait_limit{-1};
+
+// Opt k3d_tma into its dynamic shared memory (once per instantiation and
+// device: the attribute belongs to the device's context).
 template <bool MAT, bool FDIV>
 static int tma_attr() {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k3d_tma<MAT, FDIV>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(TmaSmem));
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 64) return set_error(WF_E_LIMIT, "k3d_tma: device %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_tma_mu);
+  if (!attr[dev]) {
+    e = cudaFuncSetAttribute(k3d_tma<MAT, FDIV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(TmaSmem));
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k3d_tma)");
-    attr = true;
+    attr[dev] = true;
   }
   return WF_OK;
 }
@@ -823,8 +839,10 @@ static int launch_tma(const TmaMaps& maps, const Tile3D& P, int seg_len, int n, 
   const int rc = tma_attr<MAT, FDIV>();
   if (rc != WF_OK) return rc;
   dim3 grid((unsigned)nblk, (unsigned)nb);
-  k3d_tma<MAT, FDIV><<<grid, kTJ * kTK, smem, st>>>(maps, P, tiles_j, tiles_k, seg_len, n,
-                                                     tma_status_ptr());
+  const long long lim = g_tma_wait_limit.load();
+  k3d_tma<MAT, FDIV><<<grid, kTJ * kTK, smem, st>>>(
+      maps, P, tiles_j, tiles_k, seg_len, n, tma_status_ptr(),
+      lim < 0 ? kSpinLimit : (unsigned)std::min(lim, 0xffffffffLL));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "launch k3d_tma");
   return WF_OK;
@@ -1078,6 +1096,11 @@ extern "C" int32_t wf_fdtd3d_batch_run(const wf_grid3d* g, int32_t ninst, int64_
   return run3d(g, ninst, field_stride, coef_stride, trace_stride, src_stride, f, s, ca, cb, src,
                src_per_inst, probes, nprobe, traces, trace_ld, trace_step0, step0, nsteps,
                n_check, check_max, tune, stream);
+}
+
+extern "C" int32_t wf_fdtd3d_set_wait_limit(int64_t polls) {
+  g_tma_wait_limit.store(polls < 0 ? -1LL : (long long)polls);
+  return WF_OK;
 }
 
 extern "C" int32_t wf_fdtd3d_take_status(int32_t* status) {

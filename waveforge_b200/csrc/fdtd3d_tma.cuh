@@ -20,7 +20,8 @@
 // boundary); lanes read column lane + (k0 - 1 - floor4(k0 - 1)).
 // Curl-updated H of planes f-1..f+1 and the final H of plane f live in shared
 // rows for the Mur faces and the Ampere neighbours.  Every mbarrier wait is
-// bounded: after the limit the CTA records WF_E_TIMEOUT and stops.
+// bounded: after the limit the CTA records WF_E_TIMEOUT, waits (bounded) for
+// the copies it still has in flight, and stops.
 #pragma once
 
 #include <cuda.h>
@@ -90,10 +91,37 @@ __device__ __forceinline__ void tma_load4(void* dst, const CUtensorMap* map, int
       : "memory");
 }
 
+// Non-blocking look at the slot's phase (mbarrier.test_wait never suspends).
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the phase `parity` of mbarrier b: one non-blocking look, then at
+// most `limit` hardware-suspended polls.  False = gave up (the copies it
+// waits for may still be in flight).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* b, unsigned parity,
+                                                  unsigned limit) {
+  if (mbar_test_wait(b, parity)) return true;
+  for (unsigned spin = 0; spin < limit; ++spin)
+    if (mbar_try_wait(b, parity)) return true;
+  return false;
+}
+
+// wait_limit bounds every wait of the plane pipeline (kSpinLimit in normal
+// use; a smaller value only makes the CTA give up sooner).  The final wait
+// for the copies still in flight after a give-up always uses kSpinLimit.
 template <bool MAT, bool FDIV>
 __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ TmaMaps maps,
                                                         Tile3D P, int tiles_j, int tiles_k,
-                                                        int seg_len, int n, int* status) {
+                                                        int seg_len, int n, int* status,
+                                                        unsigned wait_limit) {
   extern __shared__ __align__(128) unsigned char smraw3[];
   TmaSmem& S = *reinterpret_cast<TmaSmem*>(smraw3);
   const int nx = P.nx, ny = P.ny, nz = P.nz;
@@ -161,8 +189,10 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   }
   const int ne = S.L.ne, nh = S.L.nh;
 
+  unsigned pending = 0u;  // thread 0: slots with copies issued and not yet landed
   auto issue = [&](int p) {  // thread 0 only
     const int s = p % kRing;
+    pending |= 1u << s;
     // the slot may hold source values written by ordinary stores: order them
     // before the asynchronous-proxy overwrite
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -178,17 +208,18 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   // Wait for plane p, then add this CTA's E-source values into it: each
   // thread to its own cell, the last thread row also to the box's extra row.
   const bool in16 = w == kTJ - 1 && gj + 1 < ny && gk >= 0 && gk < nz;
+  // A wait that gives up leaves the slot's phase bit unflipped (so the drain
+  // below waits for the copy actually outstanding) and injects nothing.
   auto land = [&](int p) {
     const int s = p % kRing;
-    const unsigned par = (phase >> s) & 1u;
-    unsigned spin = 0;
-    while (!failed && !mbar_try_wait(&S.bar[s], par)) {
-      if (++spin > kSpinLimit) {
-        failed = true;
-        if (status != nullptr) atomicExch(status, WF_E_TIMEOUT);
-      }
+    if (failed) return;
+    if (!mbar_wait_bounded(&S.bar[s], (phase >> s) & 1u, wait_limit)) {
+      failed = true;
+      if (status != nullptr) atomicExch(status, WF_E_TIMEOUT);
+      return;
     }
     phase ^= 1u << s;
+    pending &= ~(1u << s);
     if (ne > 0 && (in || in16)) {
       for (int q = 0; q < ne; ++q) {
         const wf_source& Q = P.src[S.L.e[q]];
@@ -399,14 +430,13 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     }
     hprev = F3{hxF, hyF, hzF};
   }
-  // every issued plane has been waited on (planes up to plast are landed in
-  // the loop); a failed wait leaves copies in flight: wait them out, bounded
+  // without a give-up every issued plane has been landed (planes up to plast
+  // are landed in the loop); after one, thread 0 waits out the copies it
+  // issued that have not landed (its phase bits still name their phases),
+  // with the full bound, so no copy writes shared memory after the CTA exits
   if (failed && tid == 0) {
-    for (int s = 0; s < kRing; ++s) {
-      unsigned spin = 0;
-      while (!mbar_try_wait(&S.bar[s], (phase >> s) & 1u) && ++spin < kSpinLimit) {
-      }
-    }
+    for (int s = 0; s < kRing; ++s)
+      if ((pending >> s) & 1u) mbar_wait_bounded(&S.bar[s], (phase >> s) & 1u, kSpinLimit);
   }
   if (check) {
 #pragma unroll

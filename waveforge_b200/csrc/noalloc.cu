@@ -28,7 +28,10 @@ constexpr long long kMaxCells = WF_NOALLOC_MAX_CELLS;
 // Ex, Ey, Hz scratch planes, kMaxCells floats each.
 static __device__ __align__(256) float g_scratch[3 * kMaxCells];
 
-// Device address of g_scratch per device (looked up once per device).
+// Device address of g_scratch per device (looked up once per device).  It is
+// the address in the device's current CUDA context: after cudaDeviceReset
+// the cached value is stale, so a process that resets a device must reload
+// this library before calling it again.
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 float* g_addr[kMaxDevices] = {};
@@ -42,8 +45,11 @@ extern "C" int32_t wf_fdtd2d_run_noalloc(const wf_grid2d* g, float* ex, float* e
                                          int32_t step0, int32_t nsteps, int32_t n_check,
                                          uint32_t* check_max, const wf_tune* tune, void* stream) {
   if (g == nullptr) return wf::set_error(WF_E_ARG, "wf_fdtd2d_run_noalloc: null grid");
+  if (g->nx < 0 || g->ny < 0)
+    return wf::set_error(WF_E_ARG, "wf_fdtd2d_run_noalloc: negative grid size %dx%d", g->nx,
+                         g->ny);
   const long long cells = (long long)g->nx * g->ny;
-  if (g->nx < 0 || g->ny < 0 || cells > kMaxCells)
+  if (cells > kMaxCells)
     return wf::set_error(WF_E_LIMIT,
                          "wf_fdtd2d_run_noalloc: grid %dx%d has %lld cells, above the %lld-cell "
                          "limit of the built-in scratch (use wf_fdtd2d_run with your own scratch)",

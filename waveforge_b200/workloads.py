@@ -34,6 +34,27 @@ def ellipse_mask(ci: float, cj: float, a: float, b: float):
     return lambda I, J: ((I - ci) / a) ** 2 + ((J - cj) / b) ** 2 <= 1.0
 
 
+def _add_ellipse(mm, center, axes, material) -> None:
+    """An axis-aligned ellipse: the product map's primitive (which its device
+    painter also knows), or the same mask through ``add_custom`` on a map that
+    lacks it (the reference's MaterialMap, src/core/materials.py:183-198)."""
+    if hasattr(mm, "add_ellipse"):
+        mm.add_ellipse(center, axes, material)
+    else:
+        mm.add_custom(ellipse_mask(center[0], center[1], axes[0], axes[1]), material)
+
+
+def _add_shell(mm, center, outer, inner, material) -> None:
+    """Cells inside the outer ellipse and outside the inner one, as
+    ``_add_ellipse`` chooses between the primitive and ``add_custom``."""
+    if hasattr(mm, "add_shell"):
+        mm.add_shell(center, outer, inner, material)
+    else:
+        o = ellipse_mask(center[0], center[1], outer[0], outer[1])
+        i = ellipse_mask(center[0], center[1], inner[0], inner[1])
+        mm.add_custom(lambda I, J: o(I, J) & ~i(I, J), material)
+
+
 def ring_positions(n: int, radius: float, ci: float, cj: float, nx: int, ny: int,
                    margin: int = 1) -> list[tuple[int, int]]:
     """``n`` cells on a circle, rounded and clamped to [margin, N-1-margin]."""
@@ -80,7 +101,7 @@ class LossyEllipses:
             a, b = (float(v) for v in rng.uniform(20 * s, 400 * s, 2))
             er = float(rng.uniform(1.0, 60.0))
             sg = float(rng.uniform(0.0, 1.5))
-            mm.add_ellipse((ci, cj), (a, b), Material(f"ellipse{e}", er, sg))
+            _add_ellipse(mm, (ci, cj), (a, b), Material(f"ellipse{e}", er, sg))
 
     @staticmethod
     def background(Material):
@@ -121,9 +142,9 @@ class BreastPhantom:
     def paint(self, mm, Material, with_tumor: bool = True) -> None:
         c = self.side / 2.0
         A, B, sk = self.A, self.B, self.skin
-        mm.add_shell((c, c), (A, B), (A - sk, B - sk), Material("skin", 36.0, 0.8))
-        mm.add_ellipse((c, c), (A - sk, B - sk), Material("adipose", 5.0, 0.04))
-        mm.add_ellipse((c, c), (A / 2.0, B / 2.0), Material("fibroglandular", 40.0, 0.8))
+        _add_shell(mm, (c, c), (A, B), (A - sk, B - sk), Material("skin", 36.0, 0.8))
+        _add_ellipse(mm, (c, c), (A - sk, B - sk), Material("adipose", 5.0, 0.04))
+        _add_ellipse(mm, (c, c), (A / 2.0, B / 2.0), Material("fibroglandular", 40.0, 0.8))
         if with_tumor:
             mm.add_circle(self.tumor_center, self.tumor_r, Material("tumor", 55.0, 1.0))
 
@@ -195,6 +216,23 @@ class Head3D:
     @staticmethod
     def background(Material):
         return Material("background", 10.0, 0.0)
+
+
+# ---------------------------------------------------------------------------
+# seeded initial fields (full-size parity cases)
+# ---------------------------------------------------------------------------
+
+def initial_fields(seed: int, shape: tuple, comps: tuple) -> dict:
+    """Seeded float32 white-noise starting values for the named components
+    (E components with unit variance, H components scaled by 1/377 ohm), so
+    that a short run touches every cell of a full-size grid, its edges and
+    every internal block boundary of the kernels from the first step."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    for c in comps:
+        v = rng.standard_normal(shape, dtype=np.float32)
+        out[c] = v if c.startswith("E") else (v * np.float32(1.0 / 377.0)).astype(np.float32)
+    return out
 
 
 # ---------------------------------------------------------------------------
