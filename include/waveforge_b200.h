@@ -94,9 +94,11 @@ typedef struct wf_probe {
 /* Launch shape of the temporally blocked kernels. steps_per_pass = temporal
  * block depth K.  2D: tile_i x tile_j = the on-chip REGION of one CTA
  * (core + K-cell halo on each side); it selects one of the compiled
- * register layouts: 48x128 (512 threads, 12 rows each; threads = 1024 selects
- * the same region on 1024 threads of 6 rows), 64x128 (1024 threads of 8 rows),
- * 32x128, 32x64 (256), 8x32 (64).
+ * register layouts, in which one warp spans the region's width (4 adjacent
+ * columns per lane for 128-wide regions) and `threads` sets the rows per
+ * thread: 64x128 on 1024 threads (2 rows; threads = 512: 4 rows), 48x128 on
+ * 512 threads (3 rows; threads >= 768: 768 threads of 2 rows), 32x128 and
+ * 32x64 on 256 threads, 8x32 on 64.
  * 3D: tile_i x tile_j x tile_k = core cells per CTA, threads per CTA; with
  * tile_i = 0 the streaming kernels (tile_j = segment length, threads = variant). */
 typedef struct wf_tune {
@@ -257,6 +259,27 @@ int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve,
 int32_t wf_batch2d_pass(const wf_solve2d* solves, const int32_t* items, int32_t nitems,
                         int32_t parity, int32_t step_offset, int32_t k,
                         const wf_tune* tune, int32_t fastdiv, void* stream);
+
+/* ALL temporal passes of many solves in ONE persistent launch, spread over
+ * the GPU by tiles.  The pass plan is wf_fdtd2d_run's for nsteps steps at
+ * depth K = tune->steps_per_pass (every solve advances nsteps steps from its
+ * own step0; the result lands in its ex/ey/hz).  tiles: ntiles (solve index,
+ * ci0, cj0) int32 triplets, cores of (tile_i-2K) x (tile_j-2K) cells, largest
+ * solves first; nbr: 9 int32 per tile, the tile itself and the tiles of the
+ * same solve whose cores touch its region (-1 = none); done: ntiles int32 and
+ * queue[0]: zeroed by the caller.  Resident CTAs take items pass-major
+ * (item i = pass i / ntiles of tile i % ntiles); an item first waits, for at
+ * most wait_limit polls (negative = 2^24), until done[] of its 9 entries
+ * reaches its pass, and after its stores sets done[tile] = pass + 1.  A wait
+ * that gives up writes WF_E_TIMEOUT to the solve's status (the tile is not
+ * computed).  Needs 3K <= tile_i and 3K <= tile_j.  Same tile routine as
+ * wf_fdtd2d_run, so every solve is bit-identical to its plain run.  Batching
+ * is new; the reference runs one FDTD2D per transmitter
+ * (examples/brain_mimo_imaging.py:176-204). */
+int32_t wf_batch2d_queue(wf_solve2d* solves, const int32_t* tiles, int32_t ntiles,
+                         const int32_t* nbr, int32_t* done, int32_t* queue, int32_t nsteps,
+                         const wf_tune* tune, int32_t fastdiv, int64_t wait_limit,
+                         void* stream);
 
 /* Recompute and keep every state of nsteps forward steps, for ntx runs that
  * share the grid and the coefficients (e.g. the transmitters of one

@@ -592,6 +592,43 @@ def case_head3d_full(R, out, n=256, steps=30, init_seed=43, batch=1):
         **{f"sha_{c.lower()}": sha(getattr(f32, c)) for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")})
 
 
+def case_cpml_profile(R, out):
+    """The CPML profile at every sample position the product's CPML uses,
+    evaluated by the reference's own ``_pml_bsigma_at_rho`` (and its
+    ``_compute_pml_coeffs`` tables), for three grids.  The position -> depth
+    mapping (low side (D - x) / D, high side (x - (n - 1 - D)) / D, E at
+    integer cells, Hz at half cells, the last half cell outside the grid) is
+    the product's; the profile values are the reference's."""
+    B = R["boundaries"]
+    res = {}
+    for q, (n, D, dx, courant) in enumerate(((40, 8, 1e-3, 0.5), (64, 10, 0.5e-3, 0.5),
+                                             (33, 6, 2e-3, 0.9))):
+        dt = R["grid"].compute_stable_dt(dx, dx, None, courant)
+        m, Rt, kmax, amax = 3, 1e-8, 5.0, 0.05
+        smax = (m + 1) * math.log(1.0 / Rt) / (2.0 * B.ETA0 * D * dx)
+        cols = {k: [] for k in ("bE", "cE", "bH", "cH", "rhoE", "rhoH")}
+        for half, tag in ((0.0, "E"), (0.5, "H")):
+            for i in range(n):
+                x = i + half
+                rho = max((D - x) / D, (x - (n - 1 - D)) / D, 0.0)
+                if rho <= 0.0 or (half and i > n - 2):
+                    b, c, rho = 1.0, 0.0, 0.0
+                else:
+                    rho = min(rho, 1.0)
+                    _, b, c = B._pml_bsigma_at_rho(rho, smax, kmax, amax, m, dt)
+                cols["b" + tag].append(b)
+                cols["c" + tag].append(c)
+                cols["rho" + tag].append(rho)
+        for k, v in cols.items():
+            res[f"c{q}_{k}"] = np.array(v, dtype=np.float64)
+        res[f"c{q}_grid"] = np.array([n, D, dx, courant, dt])
+        ref = B._compute_pml_coeffs(D, dx, dt, torch.device("cpu"), torch.float64)
+        for name, t in zip(("bE", "cE", "bH", "cH", "sE", "sH"), ref):
+            res[f"c{q}_ref_{name}"] = t.numpy()
+    res["ncases"] = 3
+    np.savez_compressed(out / "cpml_profile.npz", **res)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True, help="root of the reference project checkout")
@@ -610,6 +647,7 @@ def main():
         "lossy_full": lambda: case_lossy_full(R, out),
         "head3d_full": lambda: case_head3d_full(R, out),
         "head3d_batch": lambda: case_head3d_full(R, out, n=128, batch=8, init_seed=47),
+        "cpml": lambda: case_cpml_profile(R, out),
         "edges2d": lambda: case_edges_2d(R, out),
         "head3d": lambda: case_head3d(R, out),
         "edges3d": lambda: case_edges_3d(R, out),

@@ -130,3 +130,30 @@ def test_cpml_rejects_batched_fields(cuda):
     g = _grid(32, cuda)
     with pytest.raises(ValueError):
         FDTD2D(g, FieldSet(g, batch_size=2), CPML(g, 4))
+
+
+def test_profile_pinned_to_reference():
+    """Every b, c sample of the CPML tables equals, after float32 rounding,
+    the reference's ``_pml_bsigma_at_rho`` at the same depth
+    (src/core/boundaries.py:32-48; fixture written by running it), and the
+    ``MurABC(pml_depth=...)`` tables equal the reference's
+    ``_compute_pml_coeffs`` (:51-112) bit for bit in float64."""
+    from conftest import golden
+    from waveforge_b200.core.boundaries import _compute_pml_coeffs
+    g = golden("cpml_profile")
+    for q in range(int(g["ncases"])):
+        n, D, dx, courant, dt = g[f"c{q}_grid"]
+        n, D = int(n), int(D)
+        grid = YeeGrid(n, n, float(dx), float(dx), courant=float(courant), device="cpu")
+        assert grid.dt == float(dt)
+        t = CPML(grid, D).tables.view(2, 6, n)
+        for ax in range(2):
+            for k, name in ((0, "bE"), (1, "cE"), (3, "bH"), (4, "cH")):
+                want = torch.from_numpy(g[f"c{q}_{name}"].astype(np.float32))
+                assert torch.equal(t[ax, k], want), (q, ax, name)
+            rho_e = torch.from_numpy(g[f"c{q}_rhoE"])
+            ik = (1.0 / (1.0 + 4.0 * rho_e ** 3)).to(torch.float32)
+            assert torch.equal(t[ax, 2], ik), (q, ax)
+        mine = _compute_pml_coeffs(D, float(dx), float(dt), torch.device("cpu"), torch.float64)
+        for name, v in zip(("bE", "cE", "bH", "cH", "sE", "sH"), mine):
+            assert np.array_equal(v.numpy(), g[f"c{q}_ref_{name}"]), (q, name)

@@ -145,11 +145,12 @@ def test_breast_mimo_alone_and_batched_bit_exact(cuda):
                                      ca.reshape(ph.side, ph.side, 1).to(cuda),
                                      cb.reshape(ph.side, ph.side, 1).to(cuda)))
             keys.append(f"p{p}_tx{tx}")
-    for mode in ("persistent", "tiled"):
+    for mode in ("persistent", "tiled", "queue"):
         for tune in (None, (3, 32, 64, 1, 0), (6, 48, 128, 1, 0), (2, 8, 32, 1, 0),
-                     (4, 48, 128, 1, 1024), (5, 48, 128, 1, 1024), (7, 64, 128, 1, 1024)):
+                     (4, 48, 128, 1, 1024), (5, 48, 128, 1, 1024), (7, 64, 128, 1, 1024),
+                     (6, 64, 128, 1, 512)):
             batch = Batch2D(solves, steps, tune=tune, mode=mode)
-            if mode == "tiled":
+            if mode != "persistent":
                 for chunk in (7, 100, 1, steps - 108):   # uneven chunks, a single-step pass
                     batch.run(chunk)
             else:
@@ -312,7 +313,7 @@ def test_batch_graph_replay_and_autotune_bit_exact(cuda):
                            [("Hz", "point", (i, i + 1, j, j + 1), wave, None)], ca, cb,
                            steps=steps)
             refs.append((sim.run(steps, record=Detectors(ant)).clone(), f.Hz.clone()))
-    for mode in ("persistent", "tiled"):
+    for mode in ("persistent", "tiled", "queue"):
         b = Batch2D(solves, steps, mode=mode)
         b.capture()
         for _ in range(2):
@@ -322,7 +323,7 @@ def test_batch_graph_replay_and_autotune_bit_exact(cuda):
                 assert torch.equal(b.traces(q), tr), (mode, q)
                 assert torch.equal(b.fields(q)[2].reshape(hz.shape), hz), (mode, q)
     auto = Batch2D(solves, steps, tune="auto")
-    assert auto.mode in ("persistent", "tiled")
+    assert auto.mode in ("persistent", "tiled", "queue")
     auto.run()
     torch.cuda.synchronize()
     for q, (tr, hz) in enumerate(refs):
@@ -330,3 +331,47 @@ def test_batch_graph_replay_and_autotune_bit_exact(cuda):
     from waveforge_b200.autotune import tune_plain2d
     t = tune_plain2d(300, 200, materials=True, device=cuda)
     assert len(t) == 5 and t[0] >= 1
+
+
+def test_tile_queue_bounded_wait_reports_timeout_then_recovers(cuda):
+    """The tile-queue kernel's neighbour waits are bounded: with every pass
+    counter preset to -1 (as if no tile had finished the previous pass) and a
+    bound of 64 polls, items give up instead of waiting for good, the solves
+    report WF_E_TIMEOUT, and the next normal run of the same batch is
+    bit-identical to the plain per-solve runs."""
+    import ctypes
+    from waveforge_b200 import _native as nat
+    g = load("breast_mimo_small")
+    steps = 60
+    wave = torch.from_numpy(g["wave"][:steps].copy())
+    solves, refs = [], []
+    for p in range(len(g["sides"])):
+        ph, ca, cb = breast_coeffs(g, p)
+        ant = ph.antennas(16)
+        i, j = ant[0]
+        grid = YeeGrid(ph.side, ph.side, float(g["dx"]), float(g["dx"]),
+                       courant=float(g["courant"]), device=cuda)
+        src = PointSource(TabulatedWaveform(wave), i, j, "Hz", grid=grid, N_steps=steps)
+        solves.append(BatchSolve(grid, SourceCollection([src]), Detectors(ant),
+                                 ca.reshape(ph.side, ph.side, 1).to(cuda),
+                                 cb.reshape(ph.side, ph.side, 1).to(cuda)))
+        sim, f = sim2d(cuda, ph.side, ph.side, float(g["dx"]), float(g["courant"]),
+                       [("Hz", "point", (i, i + 1, j, j + 1), wave, None)], ca, cb, steps=steps)
+        refs.append(sim.run(steps, record=Detectors(ant)).clone())
+    b = Batch2D(solves, steps, tune=(3, 32, 64, 1, 0), mode="queue")
+    b._upload(0, steps)
+    tiles, nbr, done = b._queue_tables()
+    done.fill_(-1)
+    b._queue.zero_()
+    nat.check(nat.load().wf_batch2d_queue(
+        b._desc_dev.data_ptr(), tiles.data_ptr(), tiles.shape[0], nbr.data_ptr(),
+        done.data_ptr(), b._queue.data_ptr(), steps, ctypes.byref(b.tune),
+        1 if b._fastdiv else 0, 64, nat.stream_handle(cuda)))
+    torch.cuda.synchronize()
+    assert nat.WF_E_TIMEOUT in b.statuses()
+    b.reset()
+    b.run()
+    torch.cuda.synchronize()
+    assert all(s == 0 for s in b.statuses())
+    for q, tr in enumerate(refs):
+        assert torch.equal(b.traces(q), tr), q

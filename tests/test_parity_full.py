@@ -6,9 +6,9 @@ float64) PyTorch loop at the full sizes the benchmarks use
 ``head3d_full``, ``head3d_batch``):
 
 * breast MIMO phantoms of sides 256, 384 and 512, 3000 steps (the benchmark's
-  run length), 16 receivers: through the plain per-solve kernel, both batched
-  scheduling modes (persistent solve queue, tile passes), the benchmark's
-  tuned shape, and a CUDA-graph replay of the whole batch;
+  run length), 16 receivers: through the plain per-solve kernel, the three
+  batched schedules (persistent solve queue, tile passes, persistent tile
+  queue), two tuned shapes, and CUDA-graph replays of the whole batch;
 * the 4096^2 lossy-ellipse scene, 100 steps from seeded random starting
   fields (every cell, edge and tile boundary is live from step one), ring
   receivers plus receivers near the source, two tile shapes;
@@ -75,16 +75,17 @@ def test_breast_full_shapes_bit_exact_all_modes(cuda):
             assert sha(batch.traces(q)) == str(g[key + "_sha_traces"]), (what, key)
             assert sha(batch.fields(q)[2]) == str(g[key + "_sha_hz"]), (what, key)
 
-    for mode in ("persistent", "tiled"):
-        for tune in (None, (6, 64, 128, 1, 1024)):
+    for mode in ("persistent", "tiled", "queue"):
+        for tune in (None, (6, 64, 128, 1, 1024), (6, 64, 128, 1, 512)):
             b = Batch2D(solves, steps, tune=tune, mode=mode)
             b.run()
             check(b, (mode, tune))
-    b = Batch2D(solves, steps, tune=(6, 64, 128, 1, 1024), mode="tiled")
-    b.capture()
-    for rep in range(2):
-        b.replay()
-        check(b, ("graph replay", rep))
+    for mode in ("tiled", "queue"):
+        b = Batch2D(solves, steps, tune=(6, 64, 128, 1, 512), mode=mode)
+        b.capture()
+        for rep in range(2):
+            b.replay()
+            check(b, ("graph replay", mode, rep))
 
 
 def _lossy_full_coeffs(g):

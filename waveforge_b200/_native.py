@@ -22,7 +22,7 @@ WF_OK, WF_E_ARG, WF_E_CUDA, WF_E_LIMIT, WF_E_DIVERGED, WF_E_TIMEOUT = range(6)
 COMP_CODE = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
 
 EXPORTED = ("wf_abi_version", "wf_last_error", "wf_check_fastdiv", "wf_fdtd2d_run",
-            "wf_fdtd2d_run_noalloc", "wf_fdtd3d_run", "wf_fdtd3d_batch_run", "wf_batch2d_run", "wf_batch2d_pass", "wf_fdtd2d_states",
+            "wf_fdtd2d_run_noalloc", "wf_fdtd3d_run", "wf_fdtd3d_batch_run", "wf_batch2d_run", "wf_batch2d_pass", "wf_batch2d_queue", "wf_fdtd2d_states",
             "wf_adjoint2d_run", "wf_material_coeffs", "wf_material_grad", "wf_paint2d", "wf_paint3d", "wf_fdtd3d_take_status", "wf_fdtd3d_set_wait_limit", "wf_cpml2d_run",
             "wf_das2d", "wf_das_travel_times", "wf_das_envelope_image")
 NOALLOC_MAX_CELLS = 1 << 20   # WF_NOALLOC_MAX_CELLS of the header
@@ -146,6 +146,9 @@ def load() -> ctypes.CDLL:
                                   c_int32, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                   c_int32, c_void_p, c_int64, c_int32, c_int32, c_int32,
                                   c_int32, c_void_p, c_void_p]
+    lib.wf_batch2d_queue.restype = c_int32
+    lib.wf_batch2d_queue.argtypes = [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p,
+                                     c_int32, c_void_p, c_int32, c_int64, c_void_p]
     lib.wf_fdtd3d_take_status.restype = c_int32
     lib.wf_fdtd3d_take_status.argtypes = [c_void_p]
     lib.wf_fdtd3d_set_wait_limit.restype = c_int32

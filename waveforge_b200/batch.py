@@ -9,7 +9,11 @@ ONE persistent launch of ``wf_batch2d_run``: resident CTAs pull solves from a
 device work queue in largest-first order and run each through its steps with
 the same tile routine as ``FDTD2D``, so every solve's traces are
 bit-identical to running it alone.  Solves that share a phantom share its
-``Ca``/``Cb`` tensors.
+``Ca``/``Cb`` tensors.  Two other schedules spread a large solve over many
+SMs: one launch per temporal pass over every solve's tiles ("tiled"), and
+one persistent launch whose CTAs pull (pass, tile) items from a device queue
+and wait, bounded, for the neighbouring tiles of the previous pass
+("queue").
 
 ``run_plain`` runs the same solves one after another through
 ``wf_fdtd2d_run`` (the plain per-solve path) for comparison.
@@ -127,6 +131,25 @@ def tile_items(shapes: Sequence[tuple[int, int]], k: int, region: tuple[int, int
     return np.concatenate(out) if out else np.zeros((0, 3), dtype=np.int32)
 
 
+def tile_neighbours(tiles: np.ndarray, k: int, region: tuple[int, int]) -> np.ndarray:
+    """(ntiles, 9) int32: for every tile of ``tile_items(.., k, ..)``, itself
+    and the tiles of the same solve whose cores touch its region (-1 = none):
+    with a core of at least k cells per side those are its 8 neighbours."""
+    rh, rw = region
+    ci, cj = rh - 2 * k, rw - 2 * k
+    index = {(int(q), int(a), int(b)): t for t, (q, a, b) in enumerate(tiles)}
+    out = np.full((len(tiles), 9), -1, dtype=np.int32)
+    for t, (q, a, b) in enumerate(tiles):
+        m = 0
+        for di in (0, -ci, ci):
+            for dj in (0, -cj, cj):
+                nb = index.get((int(q), int(a) + di, int(b) + dj))
+                if nb is not None:
+                    out[t, m] = nb
+                    m += 1
+    return out
+
+
 def run_tiled_passes(desc_dev_ptr: int, items_by_k: dict, plan: PassPlan, tune, fastdiv: bool,
                      stream: int) -> None:
     """Launch every pass of ``plan`` as one wf_batch2d_pass over its items
@@ -149,9 +172,10 @@ class Batch2D:
             # time every candidate launch shape on these solves, keep the fastest
             from .autotune import tune_batch
             mode, tune = tune_batch(solves, n_steps, device=device)
-        if mode not in ("persistent", "tiled"):
+        if mode not in ("persistent", "tiled", "queue"):
             raise ValueError("mode is 'persistent' (one CTA per solve, one launch), 'tiled' "
-                             "(one launch per pass over every solve's tiles) or 'auto'")
+                             "(one launch per pass over every solve's tiles), 'queue' (one "
+                             "persistent launch pulling (pass, tile) items) or 'auto'")
         self.mode = mode
         self._graph = None
         if not solves:
@@ -271,7 +295,7 @@ class Batch2D:
 
     def launches_per_run(self) -> int:
         """Kernel launches of one full ``run()``."""
-        if self.mode == "persistent":
+        if self.mode in ("persistent", "queue"):
             return 1
         plan = PassPlan(self.n_steps, self.depth)
         return plan.passes
@@ -285,10 +309,35 @@ class Batch2D:
         t, n = cache[k]
         return t.data_ptr(), n
 
+    def _queue_tables(self):
+        """Tiles (cores of the full depth), their neighbour lists and the
+        per-tile pass counters of the tile-queue mode, built once."""
+        if "_qt" not in self.__dict__:
+            shapes = [(s.grid.Nx, s.grid.Ny) for s in self.solves]
+            tiles = tile_items(shapes, self.depth, self.region)
+            nbr = tile_neighbours(tiles, self.depth, self.region)
+            self._qt = (torch.from_numpy(tiles).to(self.device),
+                        torch.from_numpy(nbr).to(self.device),
+                        torch.zeros(len(tiles), dtype=torch.int32, device=self.device))
+        return self._qt
+
     def launch(self) -> None:
         """Advance every solve by the uploaded step count: one persistent
-        launch ("persistent"), or one tile-queue launch per temporal pass
-        ("tiled"); either sequence can be captured in a CUDA graph."""
+        launch ("persistent": a CTA per solve; "queue": CTAs pulling
+        (pass, tile) items), or one launch per temporal pass over every
+        solve's tiles ("tiled"); each can be captured in a CUDA graph."""
+        if self.mode == "queue":
+            tiles, nbr, done = self._queue_tables()
+            done.zero_()
+            self._queue.zero_()
+            nat.check(nat.load().wf_batch2d_queue(
+                self._desc_dev.data_ptr(), tiles.data_ptr(), tiles.shape[0], nbr.data_ptr(),
+                done.data_ptr(), self._queue.data_ptr(), self._launch_nsteps,
+                None if self.tune is None else ctypes.byref(self.tune),
+                1 if self._fastdiv else 0, -1, nat.stream_handle(self.device)))
+            if PassPlan(self._launch_nsteps, self.depth).needs_copy:
+                self._state.copy_(self._scratch)
+            return
         if self.mode == "tiled":
             plan = PassPlan(self._launch_nsteps, self.depth)
             items = {plan.length(p): self._items(plan.length(p)) for p in range(plan.passes)}

@@ -120,6 +120,7 @@ class EngineBase:
         self.n_stability_checks = 0
         self._src_key = None
         self._src_table: Optional[SourceTable] = None
+        self._graphs: Optional[dict] = None  # CUDA graphs of runs (compile_step)
 
     def _check_buffer(self, step0: int, nsteps: int):
         nc = self._n_check
@@ -154,6 +155,56 @@ class EngineBase:
             self._src_table = SourceTable(injectors, self._device, allowed, dims)
             self._src_key = key
         return self._src_table
+
+    # ---- CUDA-graph replay of runs -------------------------------------
+    def compile_step(self, *, backend: str = "inductor", mode: str = "reduce-overhead") -> None:
+        """Replay runs from CUDA graphs (the counterpart of the reference's
+        ``torch.compile(mode='reduce-overhead')`` step, src/core/fdtd3d.py:
+        404-419; ``backend`` and ``mode`` are accepted and ignored).  From now
+        on the first ``run(n)`` from a given start step (with given detectors
+        and sources) is captured -- every pass launch of it, the zeroing of its
+        trace and stability buffers -- and replayed; later runs with the same
+        start step and length (e.g. after ``reset()``) replay that graph, one
+        launch instead of one per pass, with bit-identical results.  Returned
+        traces are copies (the graph owns its buffer)."""
+        self._graphs = {}
+
+    def _prepare(self) -> None:
+        """Build the device tables and scratch a run needs before it can be
+        captured (their uploads and allocations cannot happen inside a graph)."""
+
+    def _graphed(self, nsteps: int, probes, alloc_traces):
+        """Run ``_advance(nsteps, probes, traces)`` through the cached graph of
+        this (start step, length, detectors, sources); returns the traces
+        buffer owned by the graph (or None)."""
+        self._prepare()
+        start = self.steps_completed
+        key = (start, nsteps, None if probes is None else id(probes), id(self._src_table),
+               None if self._scratch is None else self._scratch.data_ptr())
+        ent = self._graphs.get(key)
+        if ent is None:
+            rec = []
+            self._process_checks = lambda buf, count, step0: rec.append((buf, count, step0))
+            graph = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream(self._device)
+            side.wait_stream(torch.cuda.current_stream(self._device))
+            try:
+                with torch.cuda.stream(side):
+                    with torch.cuda.graph(graph, stream=side, capture_error_mode="relaxed"):
+                        traces = alloc_traces()
+                        self._advance(nsteps, probes, traces)
+            finally:
+                del self._process_checks
+                self.steps_completed = start
+            torch.cuda.current_stream(self._device).wait_stream(side)
+            ent = (graph, traces, rec)
+            self._graphs[key] = ent
+        graph, traces, rec = ent
+        graph.replay()
+        self.steps_completed = start + nsteps
+        for buf, count, step0 in rec:
+            self._process_checks(buf, count, step0)
+        return traces
 
     def reset(self) -> None:
         """Zero fields and telemetry (src/core/fdtd2d.py:365-378)."""

@@ -134,6 +134,12 @@ class FDTD2D(EngineBase):
         self.steps_completed += nsteps
         self._process_checks(chk, count, step0)
 
+    def _prepare(self) -> None:
+        self._sources_table(_ALLOWED_2D, 2)
+        if self._scratch is None:
+            g = self._grid
+            self._scratch = torch.empty((3, g.Nx, g.Ny), dtype=torch.float32, device=self._device)
+
     def reset(self) -> None:
         """Zero fields and telemetry, and the CPML layer memories if any."""
         super().reset()
@@ -160,8 +166,17 @@ class FDTD2D(EngineBase):
         traces = probes = None
         if record is not None:
             probes = record.table(self._device, _ALLOWED_2D, (self._grid.Nx, self._grid.Ny, 1))
+        graphed = self._graphs is not None and not verbose and n_steps > 0 and not self._cpml
+        if graphed:
+            # captured once per (start, length, detectors), replayed afterwards
+            count = 0 if probes is None else probes.count
+            traces = self._graphed(n_steps, probes, lambda: None if probes is None else torch.zeros(
+                (count, n_steps), dtype=torch.float32, device=self._device))
+            if traces is not None:
+                traces = traces.clone()
+        elif record is not None:
             traces = torch.zeros((probes.count, n_steps), dtype=torch.float32, device=self._device)
-        done = 0
+        done = n_steps if graphed else 0
         chunk = report if verbose else n_steps
         while done < n_steps:
             ns = min(chunk, n_steps - done)

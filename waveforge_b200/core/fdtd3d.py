@@ -89,9 +89,21 @@ class FDTD3D(EngineBase):
                 raise ValueError("member_sources runs on the default 3D streaming kernel")
             self._member_sources = list(member_sources)
 
-    def compile_step(self, *, backend: str = "inductor", mode: str = "reduce-overhead") -> None:
-        """Kept for API compatibility: the step is already one fused CUDA launch."""
-        return None
+    def _prepare(self) -> None:
+        if self._member_sources is None:
+            self._sources_table(FIELD_COMPONENTS, 3)
+        else:
+            self._members_table()
+        g, f = self._grid, self._fields
+        n = g.Nx * g.Ny * g.Nz
+        stream_tune = self._tune is None or self._tune.tile_i == 0
+        if f.is_batched and stream_tune and g.Nz > 1:
+            if self._scratch is None or self._scratch.numel() != 6 * f.batch_size * n:
+                self._scratch = torch.empty((6, f.batch_size, n), dtype=torch.float32,
+                                            device=self._device)
+        elif self._scratch is None:
+            self._scratch = torch.empty((6, g.Nx, g.Ny, g.Nz), dtype=torch.float32,
+                                        device=self._device)
 
     def _members(self):
         f = self._fields
@@ -206,13 +218,22 @@ class FDTD3D(EngineBase):
         t0 = time.perf_counter()
         start = self.steps_completed
         probes = traces = None
+        shape = None
         if record is not None:
             probes = record.table(self._device, FIELD_COMPONENTS, (g.Nx, g.Ny, g.Nz))
             shape = ((self._fields.batch_size,) if self._fields.is_batched else ()) + (probes.count,
                                                                                      n_steps)
+        graphed = self._graphs is not None and not verbose and n_steps > 0
+        if graphed:
+            # captured once per (start, length, detectors), replayed afterwards
+            traces = self._graphed(n_steps, probes, lambda: None if shape is None else torch.zeros(
+                shape, dtype=torch.float32, device=self._device))
+            if traces is not None:
+                traces = traces.clone()
+        elif record is not None:
             traces = torch.zeros(shape, dtype=torch.float32, device=self._device)
         chunk = max(1, n_steps // 10) if verbose else n_steps
-        done = 0
+        done = n_steps if graphed else 0
         while done < n_steps:
             ns = min(chunk, n_steps - done)
             self._advance(ns, probes, None if traces is None else traces[..., done:])

@@ -1,5 +1,8 @@
-// batch2d.cu -- persistent batched kernel for many independent, uneven 2D
-// TM solves (e.g. every transmitter of every phantom of a MIMO study).
+// batch2d.cu -- batched kernels for many independent, uneven 2D TM solves
+// (e.g. every transmitter of every phantom of a MIMO study): a persistent
+// solve queue (k_batch2d), one launch per temporal pass over every solve's
+// tiles (k_batch_pass), and a persistent tile queue over all passes
+// (k_batch_queue).
 //
 // Resident CTAs pull solve indices from a device work queue (an atomic
 // counter over a largest-first order, i.e. LPT list scheduling) and run each
@@ -217,9 +220,196 @@ struct LaunchPassBatch {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Persistent tile queue: ONE launch for all temporal passes of many solves.
+// Resident CTAs (one per SM) pull items from a device work queue; item i is
+// pass i / ntiles of tile i % ntiles (pass-major order, tiles largest solve
+// first).  Before it runs, an item waits until its own tile and the (up to 8)
+// neighbouring tiles of its solve have finished the previous pass: their
+// cores cover this tile's region (core + k-cell halo, k <= core side), so
+// the wait covers both the data this pass reads and the buffer it overwrites
+// (the previous pass's input, still read by a neighbour until it finishes).
+// Every item an item waits for sits earlier in the queue and was therefore
+// taken by a CTA that is already running, so the waits always end; they are
+// bounded all the same (wait_limit polls, then WF_E_TIMEOUT in the solve's
+// status, the tile is skipped and still marked done so nothing waits on it).
+// Region loads go through L2 (ld.global.cg): this SM may hold lines of the
+// same buffer from an earlier pass in its L1.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <class C, bool FDIV>
+__global__ void __launch_bounds__(C::THREADS, 1) k_batch_queue(
+    wf_solve2d* __restrict__ solves, const int* __restrict__ tiles, int ntiles,
+    const int* __restrict__ nbr, int* done, int* queue, int nsteps, int K,
+    unsigned wait_limit) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TileSmem<C>& sm = *reinterpret_cast<TileSmem<C>*>(smraw);
+  __shared__ int s_item, s_ok;
+  const PassPlan plan(nsteps, K);
+  const long long nitems = (long long)ntiles * plan.passes();
+  const int ci = C::RH - 2 * K, cj = C::RW - 2 * K;  // core of every pass
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const long long it = s_item;
+    if (it >= nitems || it < 0) return;
+    const int pass = (int)(it / ntiles), tile = (int)(it - (long long)pass * ntiles);
+    const int* T = tiles + 3 * (long long)tile;
+    wf_solve2d& S = solves[T[0]];
+    // lanes 0..8 of warp 0 wait for the tile itself and its neighbours
+    if (threadIdx.x < 32) {
+      bool ok = true;
+      if (threadIdx.x < 9) {
+        const int nb = nbr[9 * (long long)tile + threadIdx.x];
+        if (nb >= 0) {
+          unsigned spin = 0;
+          while (ld_acquire_gpu(done + nb) < pass) {
+            if (spin++ >= wait_limit) {
+              ok = false;
+              break;
+            }
+            __nanosleep(128);
+          }
+        }
+      }
+      ok = __all_sync(0xffffffffu, ok);
+      if (threadIdx.x == 0) {
+        s_ok = ok ? 1 : 0;
+        if (!ok) atomicExch(&S.status, WF_E_TIMEOUT);
+      }
+    }
+    __syncthreads();
+    const bool flagged = (S.g.flags & (WF_FASTDIV_X | WF_FASTDIV_Y)) == (WF_FASTDIV_X | WF_FASTDIV_Y);
+    if (FDIV && !flagged) {
+      if (threadIdx.x == 0) atomicExch(&S.status, WF_E_ARG);
+    } else if (s_ok) {
+      Tile2D P{};
+      P.nx = S.g.nx;
+      P.ny = S.g.ny;
+      P.dh = S.g.dh;
+      P.de = S.g.de;
+      P.dx = S.g.dx;
+      P.dy = S.g.dy;
+      P.mx = S.g.mur_x;
+      P.my = S.g.mur_y;
+      P.fastdiv = S.g.flags;
+      P.ca = S.ca;
+      P.cb = S.cb;
+      P.src = S.src;
+      P.nsrc = S.nsrc;
+      P.prb = S.probes;
+      P.nprb = S.nprobe;
+      P.traces = S.traces;
+      P.trace_ld = S.trace_ld;
+      P.trace_step0 = S.trace_step0;
+      P.n_check = S.n_check;
+      P.check_max = S.check_max;
+      P.check_base = S.n_check > 0 ? S.step0 / S.n_check : 0;
+      P.status = nullptr;
+      const bool par = pass & 1;
+      P.ex_in = par ? S.sx : S.ex;
+      P.ey_in = par ? S.sy : S.ey;
+      P.hz_in = par ? S.sz : S.hz;
+      P.ex_out = par ? S.ex : S.sx;
+      P.ey_out = par ? S.ey : S.sy;
+      P.hz_out = par ? S.hz : S.sz;
+      const int ci0 = T[1], cj0 = T[2];
+      const int ci1 = min(ci0 + ci, P.nx), cj1 = min(cj0 + cj, P.ny);
+      const int s0 = S.step0 + plan.offset(pass), k = plan.len(pass);
+      if (S.ca != nullptr) tile2d<C, true, FDIV>(P, ci0, ci1, cj0, cj1, s0, k, sm);
+      else tile2d<C, false, FDIV>(P, ci0, ci1, cj0, cj1, s0, k, sm);
+    }
+    // tile2d ends with a CTA barrier after its stores: publish the pass
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release_gpu(done + tile, pass + 1);
+    }
+    __syncthreads();
+  }
+}
+
+struct LaunchQueueBatch {
+  wf_solve2d* solves;
+  const int* tiles;
+  int ntiles;
+  const int* nbr;
+  int* done;
+  int* queue;
+  int nsteps, K;
+  unsigned wait_limit;
+  bool fdiv;
+  cudaStream_t st;
+  template <class C>
+  int operator()() const {
+    return fdiv ? go<C, true>() : go<C, false>();
+  }
+  template <class C, bool FDIV>
+  int go() const {
+    const size_t smem = sizeof(TileSmem<C>);
+    cudaError_t e = cudaFuncSetAttribute(k_batch_queue<C, FDIV>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_batch_queue)");
+    int dev = 0, nsm = 0, per_sm = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_queue<C, FDIV>, C::THREADS,
+                                                      smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per_sm < 1) return set_error(WF_E_LIMIT, "wf_batch2d_queue: layout does not fit on an SM");
+    const long long nitems = (long long)ntiles * PassPlan(nsteps, K).passes();
+    const int grid = (int)std::min<long long>((long long)nsm * per_sm, nitems);
+    k_batch_queue<C, FDIV><<<grid, C::THREADS, smem, st>>>(solves, tiles, ntiles, nbr, done,
+                                                           queue, nsteps, K, wait_limit);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "launch k_batch_queue");
+    return WF_OK;
+  }
+};
+
 }  // namespace wf
 
 using namespace wf;
+
+extern "C" int32_t wf_batch2d_queue(wf_solve2d* solves, const int32_t* tiles, int32_t ntiles,
+                                    const int32_t* nbr, int32_t* done, int32_t* queue,
+                                    int32_t nsteps, const wf_tune* tune, int32_t fastdiv,
+                                    int64_t wait_limit, void* stream) {
+  if (ntiles < 0 || nsteps < 0 ||
+      (ntiles > 0 && (solves == nullptr || tiles == nullptr || nbr == nullptr ||
+                      done == nullptr || queue == nullptr)))
+    return set_error(WF_E_ARG, "wf_batch2d_queue: null pointer or negative count");
+  if (ntiles == 0 || nsteps == 0) return WF_OK;
+  wf_tune t{};
+  if (tune) {
+    t = *tune;
+  } else {
+    t.steps_per_pass = 6;
+    t.tile_i = 48;
+    t.tile_j = 128;
+  }
+  if (int rc = check_tune2d(t)) return rc;
+  const int K = t.steps_per_pass;
+  if (3 * K > t.tile_i || 3 * K > t.tile_j)
+    return set_error(WF_E_ARG,
+                     "wf_batch2d_queue: depth %d needs a core of at least %d cells per side "
+                     "(region %dx%d)", K, K, t.tile_i, t.tile_j);
+  if ((long long)ntiles * PassPlan(nsteps, K).passes() > 0x7fffffffLL)
+    return set_error(WF_E_LIMIT, "wf_batch2d_queue: more than 2^31-1 items");
+  const unsigned lim = wait_limit < 0 ? (1u << 24) : (unsigned)std::min<long long>(wait_limit, 0xffffffffLL);
+  return dispatch_cfg2d(t, LaunchQueueBatch{solves, tiles, ntiles, nbr, done, queue, nsteps, K,
+                                            lim, fastdiv != 0, (cudaStream_t)stream});
+}
 
 extern "C" int32_t wf_batch2d_run(const wf_solve2d* solves, int32_t nsolve, const int32_t* order,
                                   int32_t* queue, const wf_tune* tune, int32_t ctas_per_sm,

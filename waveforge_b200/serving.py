@@ -236,11 +236,10 @@ class Server:
         self.max_active = int(max_active_solves) if max_active_solves else 3 * nsm
         self.chunk = int(chunk_steps)
         self.max_wait_s = max_wait_s
-        # default: tiled -- depth 4 on 48 x 128 regions of the 1024-thread
-        # layout (the fastest served throughput on the Poisson stream of mixed
-        # sides); persistent -- depth 6 on the 512-thread layout
+        # default: tiled -- depth 4 on 64 x 128 regions of the 512-thread
+        # layout (4 x 4 cells per thread); persistent -- depth 6 on 48 x 128
         if tune is None:
-            tune = (4, 48, 128, 1, 1024) if mode == "tiled" else (6, 48, 128, 1, 0)
+            tune = (4, 64, 128, 1, 512) if mode == "tiled" else (6, 48, 128, 1, 0)
         self.tune = nat.WfTune(*tune)
         self.depth = self.tune.steps_per_pass
         self.region = (self.tune.tile_i, self.tune.tile_j)
