@@ -26,6 +26,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 namespace wf {
 
 // 16 thread rows (j) x 32 lanes (k); row 0 and lanes 0, 31 are halo.  The box
@@ -188,6 +190,13 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     }
   }
   const int ne = S.L.ne, nh = S.L.nh;
+  const bool check = P.check_max != nullptr && P.n_check > 0 && (n + 1) % P.n_check == 0;
+  __syncthreads();  // the probe list is complete
+  // CTAs with no source, probe or stability check of their own (the vast
+  // majority) run a specialisation without that code
+  const bool lists = ne > 0 || nh > 0 || S.L.np > 0 || check;
+  auto body = [&](auto lists_tag) {
+  constexpr bool LISTS = decltype(lists_tag)::value;
 
   unsigned pending = 0u;  // thread 0: slots with copies issued and not yet landed
   auto issue = [&](int p) {  // thread 0 only
@@ -220,7 +229,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     }
     phase ^= 1u << s;
     pending &= ~(1u << s);
-    if (ne > 0 && (in || in16)) {
+    if (LISTS && ne > 0 && (in || in16)) {
       for (int q = 0; q < ne; ++q) {
         const wf_source& Q = P.src[S.L.e[q]];
         if (p < Q.i0 || p >= Q.i1 || gk < Q.k0 || gk >= Q.k1) continue;
@@ -263,7 +272,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     const float ex_k = R[1], ey_k = R[kTileF + 1];
     const float ey_i = R1[kTileF], ez_i = R1[2 * kTileF];
     float vx = R[3 * kTileF], vy = R[4 * kTileF], vz = R[5 * kTileF];
-    for (int q = 0; q < nh; ++q) {
+    for (int q = 0; LISTS && q < nh; ++q) {
       const wf_source& Q = P.src[S.L.h[q]];
       if (p >= Q.i0 && p < Q.i1 && gj >= Q.j0 && gj < Q.j1 && gk >= Q.k0 && gk < Q.k1) {
         const float v = src3_value(Q, p, gj, gk, n);
@@ -312,7 +321,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   if (!failed) curl(f0, true);
   F3 hprev{0.f, 0.f, 0.f};
   unsigned mxb[6] = {0u, 0u, 0u, 0u, 0u, 0u};
-  const bool check = P.check_max != nullptr && P.n_check > 0 && (n + 1) % P.n_check == 0;
+  const bool chk = LISTS && check;
   const bool zf_on = nz > 1;
 
   for (int f = f0; f < ib && !failed; ++f) {
@@ -410,7 +419,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       P.out[3][o] = hxF;
       P.out[4][o] = hyF;
       P.out[5][o] = hzF;
-      const int np = min(S.L.np, kMaxLocalProbe3);
+      const int np = LISTS ? min(S.L.np, kMaxLocalProbe3) : 0;
       for (int q = 0; q < np; ++q) {
         const wf_probe& pr = P.prb[S.L.p[q]];
         if (pr.i == f && pr.j == gj && pr.k == gk) {
@@ -419,7 +428,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
           P.traces[(long long)S.L.p[q] * P.trace_ld + (n - P.trace_step0)] = v;
         }
       }
-      if (check) {
+      if (chk) {
         mxb[0] = max(mxb[0], abs_bits(ex));
         mxb[1] = max(mxb[1], abs_bits(ey));
         mxb[2] = max(mxb[2], abs_bits(ez));
@@ -438,7 +447,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     for (int s = 0; s < kRing; ++s)
       if ((pending >> s) & 1u) mbar_wait_bounded(&S.bar[s], (phase >> s) & 1u, kSpinLimit);
   }
-  if (check) {
+  if (chk) {
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
       for (int sh = 16; sh > 0; sh >>= 1) mxb[c] = max(mxb[c], __shfl_xor_sync(0xffffffffu, mxb[c], sh));
@@ -450,6 +459,9 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       atomicMax(&P.check_max[idx * 6 + tid], S.L.bmax[tid]);
     }
   }
+  };
+  if (lists) body(std::true_type{});
+  else body(std::false_type{});
 }
 
 }  // namespace wf
