@@ -39,14 +39,30 @@ def sources() -> list[Path]:
     return sorted(HERE.glob("*.cu"))
 
 
-def _deps_mtime() -> float:
-    hdrs = list(HERE.glob("*.cuh")) + list(INCLUDE.glob("*.h")) + [Path(__file__)]
-    return max(p.stat().st_mtime for p in hdrs)
+def _includes(path: Path, seen: set) -> None:
+    """The library headers a source includes, directly or through other headers."""
+    for line in path.read_text().splitlines():
+        line = line.strip()
+        if line.startswith("#include \""):
+            name = line.split('"')[1]
+            for d in (HERE, INCLUDE):
+                h = d / name
+                if h.exists() and h not in seen:
+                    seen.add(h)
+                    _includes(h, seen)
+
+
+def _deps_mtime(src: Path) -> float:
+    """Newest modification time of a source's own headers (and of this script:
+    a change of the build recipe rebuilds everything)."""
+    seen: set = set()
+    _includes(src, seen)
+    return max([p.stat().st_mtime for p in seen] + [Path(__file__).stat().st_mtime])
 
 
 def _compile(src: Path, force: bool, extra: list[str]) -> Path:
     obj = OBJDIR / (src.stem + ".o")
-    if not force and obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, _deps_mtime()):
+    if not force and obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, _deps_mtime(src)):
         return obj
     cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)

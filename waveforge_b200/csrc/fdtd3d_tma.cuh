@@ -153,6 +153,9 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   const long long PS = (long long)ny * nz;
   // output offset of this column, instance included (P.out stays unmodified)
   const long long colg = (in ? (long long)gj * nz + gk : 0) + (long long)inst * P.fstride;
+  // element offsets fit 32 bits: an array of 2^32 floats (16 GiB) times the
+  // 14 arrays a launch touches would exceed the device memory
+  const unsigned colg32 = (unsigned)colg, PS32 = (unsigned)PS;
   const float dh = P.dh, de = P.de, dx = P.dx, dy = P.dy, dz = P.dz;
   const float mx = P.mx, my = P.my, mz = P.mz;
   const double rdx = __drcp_rn((double)dx), rdy = __drcp_rn((double)dy),
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
         const float c = fsub(dv<FDIV>(fsub(hyF, hprev.y), dx, rdx), dv<FDIV>(fsub(hxF, hx_j), dy, rdy));
         ez = MAT ? fadd(fmul(cav, ez), fmul(cbv, c)) : fadd(ez, fmul(de, c));
       }
-      const long long o = (long long)f * PS + colg;
+      const unsigned o = (unsigned)f * PS32 + colg32;
       P.out[0][o] = ex;
       P.out[1][o] = ey;
       P.out[2][o] = ez;
