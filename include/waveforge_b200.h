@@ -172,6 +172,38 @@ int32_t wf_fdtd2d_run_noalloc(const wf_grid2d* g,
                               int32_t n_check, uint32_t* check_max,
                               const wf_tune* tune, void* stream);
 
+/* 2D TM grid constants of a float64 run: the reference's Python floats
+ * unrounded (src/core/fdtd2d.py:158-161, src/core/boundaries.py:177-178). */
+typedef struct wf_grid2d_f64 {
+  int32_t nx, ny;
+  double dh, de;
+  double dx, dy;
+  double mur_x, mur_y;
+} wf_grid2d_f64;
+
+/* Advance a float64 2D TM grid nsteps time steps: FDTD2D.step on a float64
+ * FieldSet (src/core/grid.py:226-239, src/core/fields.py:124-130), every
+ * operation of src/core/fdtd2d.py:219-257 and src/core/boundaries.py:237-274
+ * one IEEE float64 operation in the reference's order, one launch per
+ * operation.  A verification path, not the fast one.
+ *
+ *  ex,ey,hz     float64 state, nx*ny each, updated in place
+ *  hz_prev      caller-owned nx*ny float64 scratch (the Mur snapshot)
+ *  ca,cb        float64 per-cell coefficients, or both NULL (vacuum path)
+ *  src          as wf_fdtd2d_run, but wave and amp point at float64 tables
+ *  traces       float64, nprobe rows of trace_ld; step n -> column n-trace_step0
+ *  check_max    per-check maxima of |Ex|,|Ey|,|Hz| as float64 bits, 3 per
+ *               check, indexed as in wf_fdtd2d_run; NULL = off.  Zeroed by
+ *               the caller. */
+int32_t wf_fdtd2d_run_f64(const wf_grid2d_f64* g,
+                          double* ex, double* ey, double* hz, double* hz_prev,
+                          const double* ca, const double* cb,
+                          const wf_source* src, int32_t nsrc,
+                          const wf_probe* probes, int32_t nprobe,
+                          double* traces, int64_t trace_ld, int32_t trace_step0,
+                          int32_t step0, int32_t nsteps,
+                          int32_t n_check, uint64_t* check_max, void* stream);
+
 /* Advance a 3D grid nsteps time steps.
  * Replaces FDTD3D.step/run (src/core/fdtd3d.py:261-516) with
  * MurABC3D.snapshot/apply (src/core/boundaries.py:488-583), source injection

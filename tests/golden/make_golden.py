@@ -629,6 +629,109 @@ def case_cpml_profile(R, out):
     np.savez_compressed(out / "cpml_profile.npz", **res)
 
 
+def case_f64_2d(R, out):
+    """float64 FieldSets run by the reference's FDTD2D, with the float64
+    waveform and amplitude tables stored so the float64 engine can replay them:
+      vac   -- 160x192 vacuum; a Gaussian-derivative Hz point source, a
+               weighted Ex line source, two coincident Ey point sources and an
+               Hz point on the i=0 edge; 60 probes of all three components
+               (edges included); 700 steps; stability checks every 50 steps;
+      mat   -- the lossy-ellipse scene at 256^2, 500 steps, seeded random
+               starting fields;
+      batch -- a batched FieldSet (3 members, 64x48, different random starting
+               fields, shared Ca/Cb, one broadcast Hz point source), 300 steps.
+    Digests (SHA-256) cover the float64 traces and final fields."""
+    F = R["fields"]
+    S = R["sources"]
+    Tab = tab_class(R)
+    GD = gauss_deriv_class(R)
+    M = R["materials"].Material
+    rng = np.random.default_rng(64)
+    res = {}
+
+    # --- vac
+    nx, ny, steps = 160, 192, 700
+    grid = R["grid"].YeeGrid(nx, ny, 1e-3, 1e-3, courant=0.6, device="cpu", dtype=torch.float64)
+    f = F.FieldSet(grid)
+    b = R["boundaries"].MurABC(grid, f.Hz)
+    w0 = GD().build(steps, grid.dt, torch.device("cpu"), torch.float64)
+    w1 = torch.from_numpy(rng.standard_normal(steps))
+    w2 = torch.from_numpy(rng.standard_normal(steps))
+    w3 = torch.from_numpy(rng.standard_normal(steps))
+    amp = torch.from_numpy(rng.uniform(0.5, 2.0, 40))
+    srcs = [S.PointSource(Tab(w0), 80, 96, "Hz", grid=grid, N_steps=steps),
+            S.LineSource(Tab(w1), "x", 30, 60, 100, "Ex", grid=grid, N_steps=steps,
+                         amplitude_profile=amp),
+            S.PointSource(Tab(w2), 120, 50, "Ey", grid=grid, N_steps=steps),
+            S.PointSource(Tab(w2), 120, 50, "Ey", grid=grid, N_steps=steps),
+            S.PointSource(Tab(w3), 0, 140, "Hz", grid=grid, N_steps=steps)]
+    sim = R["fdtd2d"].FDTD2D(grid, f, b, S.SourceCollection(srcs), n_check=50)
+    pts = [(0, 0), (0, 191), (159, 0), (159, 191), (1, 96), (158, 96), (80, 0), (80, 191),
+           (80, 96), (30, 80), (120, 50), (100, 140), (0, 140), (1, 140), (45, 20),
+           (140, 170), (80, 1), (80, 190), (2, 2), (157, 189)]
+    probes = [(c, i, j) for c in ("Ex", "Ey", "Hz") for i, j in pts]
+    tr = torch.zeros(len(probes), steps, dtype=torch.float64)
+    for s in range(steps):
+        sim.step()
+        for r, (c, i, j) in enumerate(probes):
+            tr[r, s] = getattr(f, c)[i, j, 0]
+    res.update(vac_waves=torch.stack([w0, w1, w2, w3]).numpy(), vac_amp=amp.numpy(),
+               vac_probes=np.array([(("Ex", "Ey", "Hz").index(c), i, j) for c, i, j in probes]),
+               vac_sha_traces=sha(tr), vac_sha_ex=sha(f.Ex), vac_sha_ey=sha(f.Ey),
+               vac_sha_hz=sha(f.Hz), vac_traces_dec=dec(tr.numpy(), 7),
+               vac_last_max=sim.last_field_max, vac_checks=sim.n_stability_checks,
+               vac_dt=grid.dt)
+
+    # --- mat
+    n, steps = 256, 500
+    wl = W.LossyEllipses(n=n, steps=steps)
+    grid = R["grid"].YeeGrid(n, n, wl.dx, wl.dx, courant=wl.courant, device="cpu",
+                             dtype=torch.float64)
+    f = F.FieldSet(grid)
+    init = W.initial_fields(65, (n, n), ("Ex", "Ey", "Hz"))
+    for c, v in init.items():
+        getattr(f, c).copy_(torch.from_numpy(v).to(torch.float64).reshape(n, n, 1))
+    b = R["boundaries"].MurABC(grid, f.Hz)
+    mm = R["materials"].MaterialMap(grid, default=wl.background(M))
+    wl.paint(mm, M)
+    ca, cb = mm.build()
+    wave = GD().build(steps, grid.dt, torch.device("cpu"), torch.float64)
+    src = S.PointSource(Tab(wave), *wl.source, "Hz", grid=grid, N_steps=steps)
+    sim = R["fdtd2d"].FDTD2D(grid, f, b, S.SourceCollection([src]), Ca=ca, Cb=cb,
+                             n_check=10 ** 9)
+    rx = [("Hz", i, j) for i, j in wl.receivers]
+    tr = torch.zeros(len(rx), steps, dtype=torch.float64)
+    for s in range(steps):
+        sim.step()
+        for r, (c, i, j) in enumerate(rx):
+            tr[r, s] = getattr(f, c)[i, j, 0]
+    res.update(mat_n=n, mat_steps=steps, mat_seed=wl.seed, mat_init_seed=65,
+               mat_wave=wave.numpy(), mat_src=np.array(wl.source),
+               mat_rx=np.array([r[1:] for r in rx]), mat_sha_ca=sha(ca), mat_sha_cb=sha(cb),
+               mat_sha_traces=sha(tr), mat_sha_ex=sha(f.Ex), mat_sha_ey=sha(f.Ey),
+               mat_sha_hz=sha(f.Hz), mat_dt=grid.dt)
+
+    # --- batch
+    nx, ny, B, steps = 64, 48, 3, 300
+    grid = R["grid"].YeeGrid(nx, ny, 2e-3, 2e-3, courant=0.7, device="cpu", dtype=torch.float64)
+    f = F.FieldSet(grid, batch_size=B)
+    for c, v in W.initial_fields(66, (B, nx, ny), ("Ex", "Ey", "Hz")).items():
+        getattr(f, c).copy_(torch.from_numpy(v).to(torch.float64).reshape(B, nx, ny, 1))
+    b = R["boundaries"].MurABC(grid, f.Hz)
+    mm = R["materials"].MaterialMap(grid, default=M("bg", 3.0, 0.05))
+    mm.add_circle((30.0, 20.0), 9.0, M("c", 20.0, 0.8))
+    ca, cb = mm.build()
+    wave = torch.from_numpy(rng.standard_normal(steps))
+    src = S.PointSource(Tab(wave), 20, 30, "Hz", grid=grid, N_steps=steps)
+    sim = R["fdtd2d"].FDTD2D(grid, f, b, S.SourceCollection([src]), Ca=ca, Cb=cb, n_check=25)
+    for s in range(steps):
+        sim.step()
+    res.update(batch_wave=wave.numpy(), batch_sha_ca=sha(ca), batch_sha_ex=sha(f.Ex),
+               batch_sha_ey=sha(f.Ey), batch_sha_hz=sha(f.Hz), batch_last_max=sim.last_field_max,
+               batch_checks=sim.n_stability_checks)
+    np.savez_compressed(out / "f64_2d.npz", **res)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True, help="root of the reference project checkout")
@@ -648,6 +751,7 @@ def main():
         "head3d_full": lambda: case_head3d_full(R, out),
         "head3d_batch": lambda: case_head3d_full(R, out, n=128, batch=8, init_seed=47),
         "cpml": lambda: case_cpml_profile(R, out),
+        "f64": lambda: case_f64_2d(R, out),
         "edges2d": lambda: case_edges_2d(R, out),
         "head3d": lambda: case_head3d(R, out),
         "edges3d": lambda: case_edges_3d(R, out),

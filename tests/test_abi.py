@@ -43,6 +43,7 @@ def test_every_declared_entry_point_is_exported():
 
 STRUCTS = {
     "wf_grid2d": (nat.WfGrid2D, ["nx", "ny", "dh", "de", "dx", "dy", "mur_x", "mur_y", "flags"]),
+    "wf_grid2d_f64": (nat.WfGrid2DF64, ["nx", "ny", "dh", "de", "dx", "dy", "mur_x", "mur_y"]),
     "wf_grid3d": (nat.WfGrid3D, ["nx", "nz", "dh", "dz", "mur_z", "flags"]),
     "wf_source": (nat.WfSource, ["comp", "k1", "n_wave", "wave", "amp"]),
     "wf_probe": (nat.WfProbe, ["comp", "i", "j", "k"]),
@@ -82,6 +83,15 @@ def test_argument_errors_need_no_gpu():
                            0, 0, 0, 10, 0, None, None, None)
     assert rc == nat.WF_E_ARG
     assert b"4x4" in lib.wf_last_error()
+    g64 = nat.WfGrid2DF64(3, 8, 1.0, 1.0, 1.0, 1.0, -0.5, -0.5)
+    rc = lib.wf_fdtd2d_run_f64(ctypes.byref(g64), 1, 1, 1, 1, None, None, None, 0, None, 0, None,
+                               0, 0, 0, 10, 0, None, None)
+    assert rc == nat.WF_E_ARG and b"4x4" in lib.wf_last_error()
+    g64.nx = 8
+    # a trace window shorter than the run
+    rc = lib.wf_fdtd2d_run_f64(ctypes.byref(g64), 1, 1, 1, 1, None, None, None, 0, 1, 1, 1, 5,
+                               0, 0, 10, 0, None, None)
+    assert rc == nat.WF_E_ARG
     rc = lib.wf_das2d(None, None, 1, 1, None, None, None, 1, None, 1, 1.0, 1.0, 0, 0, None, None)
     assert rc == nat.WF_E_ARG
 

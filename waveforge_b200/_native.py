@@ -22,7 +22,7 @@ WF_OK, WF_E_ARG, WF_E_CUDA, WF_E_LIMIT, WF_E_DIVERGED, WF_E_TIMEOUT = range(6)
 COMP_CODE = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5}
 
 EXPORTED = ("wf_abi_version", "wf_last_error", "wf_check_fastdiv", "wf_fdtd2d_run",
-            "wf_fdtd2d_run_noalloc", "wf_fdtd3d_run", "wf_fdtd3d_batch_run", "wf_batch2d_run", "wf_batch2d_pass", "wf_batch2d_queue", "wf_fdtd2d_states",
+            "wf_fdtd2d_run_noalloc", "wf_fdtd2d_run_f64", "wf_fdtd3d_run", "wf_fdtd3d_batch_run", "wf_batch2d_run", "wf_batch2d_pass", "wf_batch2d_queue", "wf_fdtd2d_states",
             "wf_adjoint2d_run", "wf_material_coeffs", "wf_material_grad", "wf_paint2d", "wf_paint3d", "wf_fdtd3d_take_status", "wf_fdtd3d_set_wait_limit", "wf_cpml2d_run",
             "wf_das2d", "wf_das_travel_times", "wf_das_envelope_image")
 NOALLOC_MAX_CELLS = 1 << 20   # WF_NOALLOC_MAX_CELLS of the header
@@ -41,6 +41,11 @@ class WfGrid2D(ctypes.Structure):
     _fields_ = [("nx", c_int32), ("ny", c_int32), ("dh", c_float), ("de", c_float),
                 ("dx", c_float), ("dy", c_float), ("mur_x", c_float), ("mur_y", c_float),
                 ("flags", c_int32)]
+
+
+class WfGrid2DF64(ctypes.Structure):
+    _fields_ = [("nx", c_int32), ("ny", c_int32), ("dh", c_double), ("de", c_double),
+                ("dx", c_double), ("dy", c_double), ("mur_x", c_double), ("mur_y", c_double)]
 
 
 class WfGrid3D(ctypes.Structure):
@@ -106,6 +111,11 @@ def load() -> ctypes.CDLL:
         POINTER(WfGrid2D), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
         c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int32,
         c_int32, c_int32, c_int32, c_void_p, POINTER(WfTune), c_void_p]
+    lib.wf_fdtd2d_run_f64.restype = c_int32
+    lib.wf_fdtd2d_run_f64.argtypes = [
+        POINTER(WfGrid2DF64), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+        c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int64, c_int32, c_int32, c_int32,
+        c_int32, c_void_p, c_void_p]
     lib.wf_fdtd2d_run_noalloc.restype = c_int32
     lib.wf_fdtd2d_run_noalloc.argtypes = [
         POINTER(WfGrid2D), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int32,

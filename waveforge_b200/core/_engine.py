@@ -42,7 +42,7 @@ class SourceTable:
     """Device array of wf_source boxes plus the tensors they point at."""
 
     def __init__(self, injectors: Sequence, device: torch.device, allowed: Sequence[str],
-                 dims: int) -> None:
+                 dims: int, dtype: torch.dtype = torch.float32) -> None:
         boxes = []
         for inj in injectors:
             if not hasattr(inj, "native_boxes"):
@@ -56,13 +56,14 @@ class SourceTable:
                 raise KeyError(f"source component {comp!r} is not a field of the {dims}D engine "
                                f"(allowed: {tuple(allowed)})")
             wave = wave.contiguous()
-            if wave.dtype != torch.float32:
-                raise TypeError("source waveforms must be float32 on the CUDA engine")
+            if wave.dtype != dtype:
+                raise TypeError(f"source waveforms must be {dtype} (the grid dtype) on the CUDA "
+                                "engine")
             if wave.device != device:
                 wave = wave.to(device)
             self.keep.append(wave)
             if amp is not None:
-                amp = amp.to(device=device, dtype=torch.float32).contiguous()
+                amp = amp.to(device=device, dtype=dtype).contiguous()
                 self.keep.append(amp)
             arr[q] = nat.WfSource(nat.COMP_CODE[comp], i0, i1, j0, j1, k0, k1, wave.numel(),
                                   wave.data_ptr(), None if amp is None else amp.data_ptr())
@@ -109,6 +110,7 @@ class EngineBase:
     """Shared telemetry / stability bookkeeping."""
 
     _components: tuple[str, ...] = ()
+    _dtype: torch.dtype = torch.float32   # arithmetic type of fields, waves and traces
 
     def _init_common(self, stability_threshold: float, n_check: int) -> None:
         self._threshold = stability_threshold
@@ -129,13 +131,14 @@ class EngineBase:
         count = (step0 + nsteps) // nc - step0 // nc
         if count == 0:
             return None, 0
-        buf = torch.zeros(count * len(self._components), dtype=torch.int32, device=self._device)
+        bits = torch.int64 if self._dtype == torch.float64 else torch.int32
+        buf = torch.zeros(count * len(self._components), dtype=bits, device=self._device)
         return buf, count
 
     def _process_checks(self, buf: Optional[torch.Tensor], count: int, step0: int) -> None:
         if buf is None:
             return
-        vals = buf.cpu().view(torch.float32).view(count, len(self._components)).tolist()
+        vals = buf.cpu().view(self._dtype).view(count, len(self._components)).tolist()
         first = step0 // self._n_check + 1
         for c in range(count):
             self.n_stability_checks += 1
@@ -152,7 +155,7 @@ class EngineBase:
         injectors = source_list(self._sources)
         key = (id(self._sources), tuple(id(s) for s in injectors))
         if self._src_table is None or self._src_key != key:
-            self._src_table = SourceTable(injectors, self._device, allowed, dims)
+            self._src_table = SourceTable(injectors, self._device, allowed, dims, self._dtype)
             self._src_key = key
         return self._src_table
 

@@ -5,7 +5,9 @@ the reference ``FDTD2D`` (src/core/fdtd2d.py:67-423).  Each call hands a block
 of steps to ``wf_fdtd2d_run`` (fused H+Mur+injection+E+detector kernel,
 temporally blocked); fields stay in the caller's FieldSet tensors.  ``run``
 additionally accepts ``record=Detectors(...)`` to gather traces on the device
-inside the same kernels.
+inside the same kernels.  A float64 FieldSet runs ``wf_fdtd2d_run_f64``
+instead: the reference's operations one launch each, in float64, for
+verification runs.
 """
 
 from __future__ import annotations
@@ -56,8 +58,10 @@ class FDTD2D(EngineBase):
         self._device = fields.Ex.device
         for name in _ALLOWED_2D:
             nat.require_cuda(getattr(fields, name), f"FieldSet.{name}")
-        if fields.dtype != torch.float32:
-            raise TypeError("the CUDA engine computes in float32 (the reference default dtype)")
+        if fields.dtype not in (torch.float32, torch.float64):
+            raise TypeError(f"the CUDA engine computes in float32 (the reference default dtype) "
+                            f"or float64, not {fields.dtype}")
+        self._dtype = fields.dtype
         if Ca is not None:
             nat.require_cuda(Ca, "Ca")
             nat.require_cuda(Cb, "Cb")
@@ -66,11 +70,25 @@ class FDTD2D(EngineBase):
         self._cpml = bool(getattr(boundary, "is_cpml", False))
         if self._cpml and fields.is_batched:
             raise ValueError("the CPML engine runs unbatched FieldSets")
+        self._f64 = self._dtype == torch.float64
+        if self._f64 and self._cpml:
+            raise TypeError("the CPML engine computes in float32")
         mx = 0.0 if self._cpml else boundary.C_mur_x
         my = 0.0 if self._cpml else boundary.C_mur_y
-        self._g = nat.WfGrid2D(grid.Nx, grid.Ny, nat.f32(self._Dh), nat.f32(self._De),
-                               nat.f32(grid.dx), nat.f32(grid.dy), nat.f32(mx), nat.f32(my),
-                               nat.fastdiv_flags(self._device, grid.dx, grid.dy))
+        if self._f64:
+            # float64 verification path (wf_fdtd2d_run_f64): the reference's
+            # Python-float scalars unrounded; float32 Ca/Cb widen exactly, as
+            # the reference's float32 x float64 products promote them
+            self._g = nat.WfGrid2DF64(grid.Nx, grid.Ny, self._Dh, self._De, grid.dx, grid.dy,
+                                      mx, my)
+            if Ca is not None and Ca.dtype != torch.float64:
+                self._Ca, self._Cb = Ca.to(torch.float64), Cb.to(torch.float64)
+        else:
+            if Ca is not None and (Ca.dtype != torch.float32 or Cb.dtype != torch.float32):
+                raise TypeError("Ca and Cb must be float32 for a float32 FieldSet")
+            self._g = nat.WfGrid2D(grid.Nx, grid.Ny, nat.f32(self._Dh), nat.f32(self._De),
+                                   nat.f32(grid.dx), nat.f32(grid.dy), nat.f32(mx), nat.f32(my),
+                                   nat.fastdiv_flags(self._device, grid.dx, grid.dy))
         self._tune = tune_struct(tune)
         self._scratch: Optional[torch.Tensor] = None
 
@@ -96,8 +114,7 @@ class FDTD2D(EngineBase):
         step0 = self.steps_completed
         src.check_range(step0, nsteps)
         g = self._grid
-        if self._scratch is None:
-            self._scratch = torch.empty((3, g.Nx, g.Ny), dtype=torch.float32, device=self._device)
+        self._alloc_scratch()
         chk, count = self._check_buffer(step0, nsteps)
         lib = nat.load()
         stream = nat.stream_handle(self._device)
@@ -108,6 +125,16 @@ class FDTD2D(EngineBase):
             for t in (ex, ey, hz) + ((ca, cb) if ca is not None else ()):
                 if not t.is_contiguous() or t.numel() != g.Nx * g.Ny:
                     raise ValueError("field / coefficient tensors must be contiguous (Nx, Ny, 1)")
+            if self._f64:
+                nat.check(lib.wf_fdtd2d_run_f64(
+                    ctypes.byref(self._g), ex.data_ptr(), ey.data_ptr(), hz.data_ptr(),
+                    self._scratch.data_ptr(), nat.ptr(ca), nat.ptr(cb), src.ptr, src.count,
+                    None if probes is None else probes.ptr, 0 if probes is None else probes.count,
+                    None if traces is None else traces.data_ptr(),
+                    0 if traces is None else traces.stride(0), step0, step0, nsteps,
+                    self._n_check if chk is not None else 0,
+                    None if chk is None else chk.data_ptr(), stream))
+                continue
             if self._cpml:
                 bd = self._boundary
                 nat.check(lib.wf_cpml2d_run(
@@ -134,11 +161,17 @@ class FDTD2D(EngineBase):
         self.steps_completed += nsteps
         self._process_checks(chk, count, step0)
 
-    def _prepare(self) -> None:
-        self._sources_table(_ALLOWED_2D, 2)
+    def _alloc_scratch(self) -> None:
+        """Ping-pong partners of the float32 passes, or the float64 path's Mur
+        snapshot of Hz."""
         if self._scratch is None:
             g = self._grid
-            self._scratch = torch.empty((3, g.Nx, g.Ny), dtype=torch.float32, device=self._device)
+            shape = (g.Nx, g.Ny) if self._f64 else (3, g.Nx, g.Ny)
+            self._scratch = torch.empty(shape, dtype=self._dtype, device=self._device)
+
+    def _prepare(self) -> None:
+        self._sources_table(_ALLOWED_2D, 2)
+        self._alloc_scratch()
 
     def reset(self) -> None:
         """Zero fields and telemetry, and the CPML layer memories if any."""
@@ -171,11 +204,11 @@ class FDTD2D(EngineBase):
             # captured once per (start, length, detectors), replayed afterwards
             count = 0 if probes is None else probes.count
             traces = self._graphed(n_steps, probes, lambda: None if probes is None else torch.zeros(
-                (count, n_steps), dtype=torch.float32, device=self._device))
+                (count, n_steps), dtype=self._dtype, device=self._device))
             if traces is not None:
                 traces = traces.clone()
         elif record is not None:
-            traces = torch.zeros((probes.count, n_steps), dtype=torch.float32, device=self._device)
+            traces = torch.zeros((probes.count, n_steps), dtype=self._dtype, device=self._device)
         done = n_steps if graphed else 0
         chunk = report if verbose else n_steps
         while done < n_steps:
