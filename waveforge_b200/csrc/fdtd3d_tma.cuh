@@ -18,10 +18,14 @@
 // thread issues global loads, shuffles or address arithmetic for them.  The
 // box starts at k = floor4(k0 - 1) (a TMA box must start on a 16-byte
 // boundary); lanes read column lane + (k0 - 1 - floor4(k0 - 1)).
-// Curl-updated H of planes f-1..f+1 and the final H of plane f live in shared
-// rows for the Mur faces and the Ampere neighbours.  Every mbarrier wait is
-// bounded: after the limit the CTA records WF_E_TIMEOUT, waits (bounded) for
-// the copies it still has in flight, and stops.
+// Curl-updated H of planes f and f+1 live in shared rows for the Mur faces and
+// the Ampere neighbours (the final H of plane f too, on x-face planes).
+// Column blocks that touch no domain face run interior planes straight-line
+// (no neighbour tests; ring slots fixed at compile time; halo threads compute
+// and do not store); blocks on a j or k face correct their face cells in
+// place.  Every mbarrier wait is bounded: after the limit the CTA records
+// WF_E_TIMEOUT, waits (bounded) for the copies it still has in flight, and
+// stops.
 #pragma once
 
 #include <cuda.h>
@@ -50,7 +54,7 @@ struct TmaMaps {
 
 struct TmaSmem {
   float raw[kRing][8][kTileF];      // slot, array, row * kBoxK + column
-  float hc[3][3][kTJ][kTK];         // curl-updated H of planes (p mod 3)
+  float hc[2][3][kTJ][kTK];         // curl-updated H of planes (p mod 2)
   float hf[3][kTJ][kTK];            // final H of plane f
   float hom[2][kTJ][kTK];           // old Hy, Hz of plane Nx-2 (x face at Nx-1)
   unsigned long long bar[kRing];
@@ -256,12 +260,16 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
   // a block none of whose cells lies on a j or k face needs the Mur code only
   // on the planes i = 0 and i = Nx - 1
   const bool face_blk = !(j0 >= 1 && j0 + kTJ - 1 <= ny - 2 && k0 >= 1 && k0 + kTK - 1 <= nz - 2);
+  // j/k face cells of this thread (the in-place face path needs the cells
+  // next to a face to be off every face: ny, nz >= 4)
+  const bool lite_ok = ny >= 4 && nz >= 4;
+  const bool on_face = (gj == 0 || gj == ny - 1) || (nz > 1 && in && (gk == 0 || gk == nz - 1));
   // carried between planes: Ey, Ez of plane p (read as the i + 1 neighbours
   // of plane p - 1), E, Ca, Cb of the plane being finished, curl-updated H
   float cey = 0.f, cez = 0.f, cca = 0.f, ccb = 0.f;
   F3 ecur{0.f, 0.f, 0.f}, hcur{0.f, 0.f, 0.f};
 
-  // Faraday update of plane p into S.hc[p % 3] (all region cells); E, Ca, Cb
+  // Faraday update of plane p into S.hc[p % 2] (all region cells); E, Ca, Cb
   // of plane p are left in ecur, cca, ccb, the curl-updated H in hcur.
   auto curl = [&](int p, bool first) {
     const float* R = raw0 + (p & (kRing - 1)) * kSlotF;
@@ -284,23 +292,29 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
         else vz = fadd(vz, v);
       }
     }
+    // every operand read below lies inside the staged boxes, so the three
+    // updates run unconditionally and cells without the neighbour keep the
+    // old value (a select, no branch)
     const bool il = p < nx - 1;
-    if (cjk) {
+    {
       const float t1 = dv<FDIV>(fsub(ey_k, ey), dz, rdz);
       const float t2 = dv<FDIV>(fsub(ez_j, ez), dy, rdy);
-      vx = fadd(vx, fmul(dh, fsub(t1, t2)));
+      const float v = fadd(vx, fmul(dh, fsub(t1, t2)));
+      vx = cjk ? v : vx;
     }
-    if (il && ck) {
+    {
       const float t1 = dv<FDIV>(fsub(ez_i, ez), dx, rdx);
       const float t2 = dv<FDIV>(fsub(ex_k, ex), dz, rdz);
-      vy = fadd(vy, fmul(dh, fsub(t1, t2)));
+      const float v = fadd(vy, fmul(dh, fsub(t1, t2)));
+      vy = (il && ck) ? v : vy;
     }
-    if (il && cj) {
+    {
       const float t1 = dv<FDIV>(fsub(ex_j, ex), dy, rdy);
       const float t2 = dv<FDIV>(fsub(ey_i, ey), dx, rdx);
-      vz = fadd(vz, fmul(dh, fsub(t1, t2)));
+      const float v = fadd(vz, fmul(dh, fsub(t1, t2)));
+      vz = (il && cj) ? v : vz;
     }
-    float* H = hc0 + (p % 3) * kHcSetF;
+    float* H = hc0 + (p & 1) * kHcSetF;
     H[0] = vx;
     H[kHcF] = vy;
     H[2 * kHcF] = vz;
@@ -335,26 +349,87 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     failed = __syncthreads_or(failed) != 0;
     if (failed) break;
     const bool face = face_blk || f == 0 || f == nx - 1;  // uniform over the CTA
+    // j/k faces only (no x face on this plane, and plane f is not the one the
+    // x face at Nx-1 reads): face cells fix their H in place in hc(f)
+    const bool face_lite = lite_ok && f >= 1 && f + 2 < nx;
     // plane f's slot takes plane f + 4 once nothing reads it: right after
     // barrier A (Ca, Cb and E of plane f are in registers; the old H of plane
     // Nx - 2 is read below, but no plane is issued then) unless the Mur code
     // reads plane f's old H, then after barrier C
     if (!face && tid == 0 && f + kRing <= plast) issue(f + kRing);
+    // Interior column block, interior plane, no sources / probes / check: every
+    // neighbour exists, so the update runs straight-line; halo threads compute
+    // too and only core threads store.
+    if (!LISTS && !face_blk && f >= ia && f >= 1 && f + 2 < nx) {
+     auto fastp = [&](auto s_tag) {
+      constexpr int SF = decltype(s_tag)::value;  // f & 3
+      const float* R = raw0 + ((SF + 1) & (kRing - 1)) * kSlotF;
+      const float* R1 = raw0 + ((SF + 2) & (kRing - 1)) * kSlotF;
+      const float ex = R[0], ey = cey, ez = cez;
+      const float ex_j = R[kBoxK], ez_j = R[2 * kTileF + kBoxK];
+      const float ex_k = R[1], ey_k = R[kTileF + 1];
+      const float ey_i = R1[kTileF], ez_i = R1[2 * kTileF];
+      float vx = R[3 * kTileF], vy = R[4 * kTileF], vz = R[5 * kTileF];
+      vx = fadd(vx, fmul(dh, fsub(dv<FDIV>(fsub(ey_k, ey), dz, rdz), dv<FDIV>(fsub(ez_j, ez), dy, rdy))));
+      vy = fadd(vy, fmul(dh, fsub(dv<FDIV>(fsub(ez_i, ez), dx, rdx), dv<FDIV>(fsub(ex_k, ex), dz, rdz))));
+      vz = fadd(vz, fmul(dh, fsub(dv<FDIV>(fsub(ex_j, ex), dy, rdy), dv<FDIV>(fsub(ey_i, ey), dx, rdx))));
+      float* H = hc0 + ((SF + 1) & 1) * kHcSetF;
+      H[0] = vx;
+      H[kHcF] = vy;
+      H[2 * kHcF] = vz;
+      // Ampere of plane f from the curl-updated (= final) H of plane f
+      const float* N = hc0 + (SF & 1) * kHcSetF;
+      const float hz_j = N[2 * kHcF - kTK], hx_j = N[-kTK];
+      const float hy_k = N[kHcF - 1], hx_k = N[-1];
+      const float hxF = hcur.x, hyF = hcur.y, hzF = hcur.z;
+      const float t1 = fsub(dv<FDIV>(fsub(hzF, hz_j), dy, rdy), dv<FDIV>(fsub(hyF, hy_k), dz, rdz));
+      const float t2 = fsub(dv<FDIV>(fsub(hxF, hx_k), dz, rdz), dv<FDIV>(fsub(hzF, hprev.z), dx, rdx));
+      const float t3 = fsub(dv<FDIV>(fsub(hyF, hprev.y), dx, rdx), dv<FDIV>(fsub(hxF, hx_j), dy, rdy));
+      const float exn = MAT ? fadd(fmul(cca, ecur.x), fmul(ccb, t1)) : fadd(ecur.x, fmul(de, t1));
+      const float eyn = MAT ? fadd(fmul(cca, ecur.y), fmul(ccb, t2)) : fadd(ecur.y, fmul(de, t2));
+      const float ezn = MAT ? fadd(fmul(cca, ecur.z), fmul(ccb, t3)) : fadd(ecur.z, fmul(de, t3));
+      if (core) {
+        const unsigned o = (unsigned)f * PS32 + colg32;
+        P.out[0][o] = exn;
+        P.out[1][o] = eyn;
+        P.out[2][o] = ezn;
+        P.out[3][o] = hxF;
+        P.out[4][o] = hyF;
+        P.out[5][o] = hzF;
+      }
+      hprev = hcur;
+      ecur = F3{ex, ey, ez};
+      hcur = F3{vx, vy, vz};
+      if (MAT) {
+        cca = R[6 * kTileF];
+        ccb = R[7 * kTileF];
+      }
+      cey = ey_i;
+      cez = ez_i;
+     };
+      switch (f & 3) {
+        case 0: fastp(std::integral_constant<int, 0>{}); break;
+        case 1: fastp(std::integral_constant<int, 1>{}); break;
+        case 2: fastp(std::integral_constant<int, 2>{}); break;
+        default: fastp(std::integral_constant<int, 3>{}); break;
+      }
+      continue;
+    }
     const F3 ef = ecur;  // E of plane f (sources included)
     const float cav = cca, cbv = ccb;
     float hxF = hcur.x, hyF = hcur.y, hzF = hcur.z;
     if (p < nx) curl(p, false);
-    const int sf = f & (kRing - 1), hf0 = f % 3;
+    const int sf = f & (kRing - 1), hf0 = f & 1;
     auto Ho = [&](int c, int ww, int ll) -> float { return S.raw[sf][3 + c][ww * kBoxK + ll + cofs]; };
     if (f == nx - 2) {
       S.hom[0][w][lane] = Ho(1, w, lane);
       S.hom[1][w][lane] = Ho(2, w, lane);
     }
     const float* Hn;  // final H of plane f, row-major [3][kTJ][kTK]
-    if (face) {
+    if (face && !face_lite) {
       __syncthreads();  // B: hc(p) visible
       // ---- Mur faces of plane f, as pure functions of old and curl-updated H ----
-      const int sp = p & (kRing - 1), hp = p % 3, hm = (f + 2) % 3;
+      const int sp = p & (kRing - 1), hp = p & 1, hm = (f + 1) & 1;
       auto Hc = [&](int c, int ww, int ll) -> float { return S.hc[hf0][c][ww][ll]; };
       // Hy, Hz after the x faces
       auto xf = [&](int c, int ww, int ll) -> float {
@@ -392,29 +467,74 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       __syncthreads();  // C: final H of plane f visible; plane f's slot unread
       if (tid == 0 && f + kRing <= plast) issue(f + kRing);
       Hn = &S.hf[0][0][0];
+    } else if (face) {
+      // Mur y and z faces of plane f, in place: the face cells read hc(f)
+      // and plane f's old H, a barrier, then they write their final H over
+      // hc(f).  Plane f is not the plane the x face at Nx-1 reads later
+      // (f + 2 < nx), so its curl-updated values are not needed again.
+      auto Hc = [&](int c, int ww, int ll) -> float { return S.hc[hf0][c][ww][ll]; };
+      auto yfx = [&](int ww, int ll) -> float {
+        const int g = j0 + ww;
+        if (g == 0 && ww + 1 < kTJ) return fadd(Ho(0, ww + 1, ll), fmul(my, fsub(Hc(0, ww + 1, ll), Ho(0, ww, ll))));
+        if (g == ny - 1 && ww >= 1) return fadd(Ho(0, ww - 1, ll), fmul(my, fsub(Hc(0, ww - 1, ll), Ho(0, ww, ll))));
+        return Hc(0, ww, ll);
+      };
+      if (on_face) {
+        if (gj == 0 && w + 1 < kTJ) {
+          hxF = fadd(Ho(0, w + 1, lane), fmul(my, fsub(Hc(0, w + 1, lane), Ho(0, w, lane))));
+          hzF = fadd(Ho(2, w + 1, lane), fmul(my, fsub(Hc(2, w + 1, lane), Ho(2, w, lane))));
+        } else if (gj == ny - 1 && w >= 1) {
+          hxF = fadd(Ho(0, w - 1, lane), fmul(my, fsub(Hc(0, w - 1, lane), Ho(0, w, lane))));
+          hzF = fadd(Ho(2, w - 1, lane), fmul(my, fsub(Hc(2, w - 1, lane), Ho(2, w, lane))));
+        }
+        if (zf_on && in) {
+          if (gk == 0 && lane + 1 < kTK) {
+            hxF = fadd(Ho(0, w, lane + 1), fmul(mz, fsub(yfx(w, lane + 1), Ho(0, w, lane))));
+            hyF = fadd(Ho(1, w, lane + 1), fmul(mz, fsub(Hc(1, w, lane + 1), Ho(1, w, lane))));
+          } else if (gk == nz - 1 && lane >= 1) {
+            hxF = fadd(Ho(0, w, lane - 1), fmul(mz, fsub(yfx(w, lane - 1), Ho(0, w, lane))));
+            hyF = fadd(Ho(1, w, lane - 1), fmul(mz, fsub(Hc(1, w, lane - 1), Ho(1, w, lane))));
+          }
+        }
+      }
+      __syncthreads();  // every correction has read what it needs
+      if (on_face) {
+        S.hc[hf0][0][w][lane] = hxF;
+        S.hc[hf0][1][w][lane] = hyF;
+        S.hc[hf0][2][w][lane] = hzF;
+      }
+      __syncthreads();  // C: final H of plane f visible; plane f's slot unread
+      if (tid == 0 && f + kRing <= plast) issue(f + kRing);
+      Hn = &S.hc[hf0][0][0][0];
     } else {
       // no face touches this block on this plane: the final H is the
       // curl-updated H, already visible since barrier A
       Hn = &S.hc[hf0][0][0][0];
     }
     // ---- Ampere update and outputs of plane f ----
-    if (f >= ia && core) {
+    {
+      // halo threads read neighbours of the row / column before their own
+      // (still inside shared memory) and store nothing
       const float* N = Hn + (w * kTK + lane);
       const float hz_j = N[2 * kHcF - kTK], hx_j = N[-kTK];
       const float hy_k = N[kHcF - 1], hx_k = N[-1];
       float ex = ef.x, ey = ef.y, ez = ef.z;
-      if (gj >= 1 && gk >= 1) {
+      {
         const float c = fsub(dv<FDIV>(fsub(hzF, hz_j), dy, rdy), dv<FDIV>(fsub(hyF, hy_k), dz, rdz));
-        ex = MAT ? fadd(fmul(cav, ex), fmul(cbv, c)) : fadd(ex, fmul(de, c));
+        const float v = MAT ? fadd(fmul(cav, ex), fmul(cbv, c)) : fadd(ex, fmul(de, c));
+        ex = (gj >= 1 && gk >= 1) ? v : ex;
       }
-      if (f >= 1 && gk >= 1) {
+      {
         const float c = fsub(dv<FDIV>(fsub(hxF, hx_k), dz, rdz), dv<FDIV>(fsub(hzF, hprev.z), dx, rdx));
-        ey = MAT ? fadd(fmul(cav, ey), fmul(cbv, c)) : fadd(ey, fmul(de, c));
+        const float v = MAT ? fadd(fmul(cav, ey), fmul(cbv, c)) : fadd(ey, fmul(de, c));
+        ey = (f >= 1 && gk >= 1) ? v : ey;
       }
-      if (f >= 1 && gj >= 1) {
+      {
         const float c = fsub(dv<FDIV>(fsub(hyF, hprev.y), dx, rdx), dv<FDIV>(fsub(hxF, hx_j), dy, rdy));
-        ez = MAT ? fadd(fmul(cav, ez), fmul(cbv, c)) : fadd(ez, fmul(de, c));
+        const float v = MAT ? fadd(fmul(cav, ez), fmul(cbv, c)) : fadd(ez, fmul(de, c));
+        ez = (f >= 1 && gj >= 1) ? v : ez;
       }
+     if (f >= ia && core) {
       const unsigned o = (unsigned)f * PS32 + colg32;
       P.out[0][o] = ex;
       P.out[1][o] = ey;
@@ -439,6 +559,7 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
         mxb[4] = max(mxb[4], abs_bits(hyF));
         mxb[5] = max(mxb[5], abs_bits(hzF));
       }
+     }
     }
     hprev = F3{hxF, hyF, hzF};
   }
