@@ -235,3 +235,51 @@ def test_member_sources_validation(cuda):
     sim = FDTD3D(g, f, b, member_sources=[one, two])                           # box counts differ
     with pytest.raises(ValueError):
         sim.run(2)
+
+
+@pytest.mark.parametrize("shape", [(40, 48, 64), (50, 33, 68), (34, 4, 8), (21, 5, 12),
+                                   (17, 21, 4)])
+def test_tma_pass_paths_bit_exact_vs_oracle(cuda, shape):
+    """Shapes that reach every path of the TMA pass: column blocks off every
+    face (straight-line interior planes; (40, 48, 64) and (50, 33, 68) have
+    them), blocks on j / k faces (in-place face corrections, down to the
+    smallest ny and nz the engine takes), x-face planes (final-H copy),
+    several i-segments (segments of 16 and of 5
+    planes besides the automatic length), sources and probes inside an
+    interior block and on faces (the list path), and stability checks every
+    3 steps (the list path on every block)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(nx * 10000 + ny * 100 + nz)
+    steps = 14
+    ca = torch.from_numpy(rng.uniform(0.3, 1.0, shape).astype(np.float32))
+    cb = torch.from_numpy(rng.uniform(0.001, 0.1, shape).astype(np.float32))
+    pts = [(nx // 2, ny // 2, nz // 2), (nx // 2, min(20, ny - 1), min(40, nz - 1)),
+           (0, ny - 1, 0), (nx - 1, 0, nz - 1), (1, 1, nz - 2)]
+    srcs = [(COMPS[q % 6], (i, i + 1, j, j + 1, k, k + 1),
+             torch.from_numpy(rng.standard_normal(steps).astype(np.float32)))
+            for q, (i, j, k) in enumerate(pts)]
+    init = {c: rng.standard_normal(shape).astype(np.float32) * (1.0 if c[0] == "E" else 2.7e-3)
+            for c in COMPS}
+    dt = oracle.stable_dt(1e-3, 1e-3, 1e-3, 0.9)
+    o = oracle.Oracle3D(nx, ny, nz, 1e-3, 1e-3, 1e-3, dt, ca, cb)
+    for c, v in init.items():
+        getattr(o, c).copy_(torch.from_numpy(v))
+    for c, box, w in srcs:
+        o.add_box_source(c, box, w)
+    probes = [(COMPS[q % 6], min(nx - 1, int(a)), min(ny - 1, int(b)), min(nz - 1, int(d)))
+              for q, (a, b, d) in enumerate(pts + [(nx // 3, ny - 2, 1), (nx - 2, 2, nz // 3)])]
+    tr_o = o.run(steps, probes)
+    for tune in (None, (1, 0, 16, 0, 0), (1, 0, 5, 0, 0)):
+        g = YeeGrid(nx, ny, 1e-3, 1e-3, Nz=nz, dz=1e-3, courant=0.9, device=cuda)
+        f = FieldSet(g)
+        for c, v in init.items():
+            getattr(f, c).copy_(torch.from_numpy(v))
+        sc = SourceCollection([PointSource(TabulatedWaveform(w), box[0], box[2], c, k=box[4], grid=g,
+                                           N_steps=steps) for c, box, w in srcs])
+        sim = FDTD3D(g, f, MurABC3D(g, f.Hx, f.Hy, f.Hz), sc, Ca=ca.to(cuda), Cb=cb.to(cuda),
+                     n_check=3, tune=tune)
+        tr = sim.run(steps, record=Detectors(probes))
+        assert np.array_equal(tr.cpu().numpy(), tr_o.numpy()), tune
+        for c in COMPS:
+            assert np.array_equal(getattr(f, c).cpu().numpy(), getattr(o, c).numpy()), (tune, c)
+        assert sim.n_stability_checks == steps // 3
