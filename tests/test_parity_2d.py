@@ -146,12 +146,9 @@ def test_breast_mimo_alone_and_batched_bit_exact(cuda):
                                      cb.reshape(ph.side, ph.side, 1).to(cuda)))
             keys.append(f"p{p}_tx{tx}")
     for mode in ("persistent", "tiled", "queue"):
-        # tile_k == 2: tile passes on persistent CTAs that stage the next
-        # tile's region in shared memory while computing (tiled mode)
         for tune in (None, (3, 32, 64, 1, 0), (6, 48, 128, 1, 0), (2, 8, 32, 1, 0),
                      (4, 48, 128, 1, 1024), (5, 48, 128, 1, 1024), (7, 64, 128, 1, 1024),
-                     (6, 64, 128, 1, 512), (8, 64, 128, 2, 512), (3, 32, 64, 2, 0),
-                     (2, 8, 32, 2, 0), (5, 48, 128, 2, 1024)):
+                     (6, 64, 128, 1, 512)):
             batch = Batch2D(solves, steps, tune=tune, mode=mode)
             if mode != "persistent":
                 for chunk in (7, 100, 1, steps - 108):   # uneven chunks, a single-step pass

@@ -193,123 +193,11 @@ __global__ void __launch_bounds__(C::THREADS, 1) k_batch_pass(const wf_solve2d* 
   else tile2d<C, false, FDIV>(P, ci0, ci1, cj0, cj1, s0, k, sm);
 }
 
-// The same pass with persistent CTAs (one per SM): CTA c runs items c, c + G,
-// c + 2G, ... of the pass (G = grid size) and, while it computes one tile,
-// stages the next tile's Ex, Ey, Hz region in shared memory with asynchronous
-// copies, so the global-load latency of a region is hidden behind the steps
-// of the previous tile.  Items of one pass are independent (the pass reads one
-// buffer set and writes the other), so no ordering between CTAs is needed.
-template <class C>
-__device__ __forceinline__ void pass_item(const wf_solve2d* __restrict__ solves,
-                                          const int* __restrict__ items, int item, int parity,
-                                          int k, Tile2D& P, int& ci0, int& ci1, int& cj0,
-                                          int& cj1, TileNext& Q, const wf_solve2d*& Sp) {
-  const int* it = items + 3 * (long long)item;
-  const wf_solve2d& S = solves[it[0]];
-  Sp = &S;
-  ci0 = it[1];
-  cj0 = it[2];
-  P = Tile2D{};
-  P.nx = S.g.nx;
-  P.ny = S.g.ny;
-  P.dh = S.g.dh;
-  P.de = S.g.de;
-  P.dx = S.g.dx;
-  P.dy = S.g.dy;
-  P.mx = S.g.mur_x;
-  P.my = S.g.mur_y;
-  P.fastdiv = S.g.flags;
-  P.ca = S.ca;
-  P.cb = S.cb;
-  P.src = S.src;
-  P.nsrc = S.nsrc;
-  P.prb = S.probes;
-  P.nprb = S.nprobe;
-  P.traces = S.traces;
-  P.trace_ld = S.trace_ld;
-  P.trace_step0 = S.trace_step0;
-  P.n_check = S.n_check;
-  P.check_max = S.check_max;
-  P.check_base = S.n_check > 0 ? S.step0 / S.n_check : 0;
-  P.status = nullptr;
-  const float* A[3] = {S.ex, S.ey, S.hz};
-  const float* B[3] = {S.sx, S.sy, S.sz};
-  P.ex_in = parity ? B[0] : A[0];
-  P.ey_in = parity ? B[1] : A[1];
-  P.hz_in = parity ? B[2] : A[2];
-  P.ex_out = const_cast<float*>(parity ? A[0] : B[0]);
-  P.ey_out = const_cast<float*>(parity ? A[1] : B[1]);
-  P.hz_out = const_cast<float*>(parity ? A[2] : B[2]);
-  const int ci = C::RH - 2 * k, cj = C::RW - 2 * k;
-  ci1 = min(ci0 + ci, P.nx);
-  cj1 = min(cj0 + cj, P.ny);
-  // the region tile2d loads (core plus k-cell halo, clipped to the domain)
-  Q.ex = P.ex_in;
-  Q.ey = P.ey_in;
-  Q.hz = P.hz_in;
-  Q.ri0 = max(ci0 - k, 0);
-  Q.rj0 = max(cj0 - k, 0);
-  Q.RHa = min(ci1 + k, P.nx) - Q.ri0;
-  Q.RWa = min(cj1 + k, P.ny) - Q.rj0;
-  Q.ny = P.ny;
-}
-
-template <class C>
-constexpr size_t pf_buf_offset() {
-  return (sizeof(TileSmem<C>) + 15) / 16 * 16;
-}
-
-template <class C, bool FDIV>
-__global__ void __launch_bounds__(C::THREADS, 1) k_batch_pass_pf(const wf_solve2d* __restrict__ solves,
-                                                                 const int* __restrict__ items,
-                                                                 int nitems, int parity, int s_off,
-                                                                 int k) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  TileSmem<C>& sm = *reinterpret_cast<TileSmem<C>*>(smraw);
-  TileBuf<C>& buf = *reinterpret_cast<TileBuf<C>*>(smraw + pf_buf_offset<C>());
-  int item = blockIdx.x;
-  if (item >= nitems) return;
-  // stage item `it`'s region into buf (only what locates the region is read)
-  auto stage = [&](int it) {
-    const int* t = items + 3 * (long long)it;
-    const wf_solve2d& Sn = solves[t[0]];
-    const int nx = Sn.g.nx, ny = Sn.g.ny, ci0 = t[1], cj0 = t[2];
-    const int ci1 = min(ci0 + C::RH - 2 * k, nx), cj1 = min(cj0 + C::RW - 2 * k, ny);
-    TileNext Qn;
-    Qn.ex = parity ? Sn.sx : Sn.ex;
-    Qn.ey = parity ? Sn.sy : Sn.ey;
-    Qn.hz = parity ? Sn.sz : Sn.hz;
-    Qn.ri0 = max(ci0 - k, 0);
-    Qn.rj0 = max(cj0 - k, 0);
-    Qn.RHa = min(ci1 + k, nx) - Qn.ri0;
-    Qn.RWa = min(cj1 + k, ny) - Qn.rj0;
-    Qn.ny = ny;
-    tile_prefetch<C>(Qn, buf);
-  };
-  stage(item);
-  for (; item < nitems; item += gridDim.x) {
-    Tile2D P;
-    TileNext Q;
-    int ci0, ci1, cj0, cj1;
-    const wf_solve2d* S;
-    pass_item<C>(solves, items, item, parity, k, P, ci0, ci1, cj0, cj1, Q, S);
-    const int nxt = item + gridDim.x;
-    auto stage_next = [&]() {
-      if (nxt < nitems) stage(nxt);
-    };
-    cp_async_wait_all();
-    __syncthreads();  // this tile's region is in buf for every thread
-    const int s0 = S->step0 + s_off;
-    if (S->ca != nullptr) tile2d<C, true, FDIV, true>(P, ci0, ci1, cj0, cj1, s0, k, sm, &buf, stage_next);
-    else tile2d<C, false, FDIV, true>(P, ci0, ci1, cj0, cj1, s0, k, sm, &buf, stage_next);
-  }
-}
-
 struct LaunchPassBatch {
   const wf_solve2d* solves;
   const int* items;
   int nitems, parity, s_off, k;
-  bool fdiv, pf;
+  bool fdiv;
   cudaStream_t st;
   template <class C>
   int operator()() const {
@@ -317,7 +205,6 @@ struct LaunchPassBatch {
   }
   template <class C, bool FDIV>
   int go() const {
-    if (pf) return go_pf<C, FDIV>();
     const size_t smem = sizeof(TileSmem<C>);
     static bool attr_done = false;
     if (!attr_done) {
@@ -329,28 +216,6 @@ struct LaunchPassBatch {
     k_batch_pass<C, FDIV><<<nitems, C::THREADS, smem, st>>>(solves, items, parity, s_off, k);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "launch k_batch_pass");
-    return WF_OK;
-  }
-  template <class C, bool FDIV>
-  int go_pf() const {
-    const size_t smem = pf_buf_offset<C>() + sizeof(TileBuf<C>);
-    static bool attr_done[64] = {false};
-    int dev = 0, nsm = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= 64) return set_error(WF_E_LIMIT, "k_batch_pass_pf: device %d out of range", dev);
-    if (!attr_done[dev]) {
-      e = cudaFuncSetAttribute(k_batch_pass_pf<C, FDIV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_batch_pass_pf)");
-      attr_done[dev] = true;
-    }
-    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
-    const int grid = std::min(nitems, std::max(1, nsm));
-    k_batch_pass_pf<C, FDIV><<<grid, C::THREADS, smem, st>>>(solves, items, nitems, parity, s_off, k);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "launch k_batch_pass_pf");
     return WF_OK;
   }
 };
@@ -588,7 +453,6 @@ extern "C" int32_t wf_batch2d_pass(const wf_solve2d* solves, const int32_t* item
   }
   t.steps_per_pass = k;
   if (int rc = check_tune2d(t)) return rc;
-  // tile_k == 2: persistent CTAs that stage the next tile while computing
   return dispatch_cfg2d(t, LaunchPassBatch{solves, items, nitems, parity, step_offset, k,
-                                           fastdiv != 0, t.tile_k == 2, (cudaStream_t)stream});
+                                           fastdiv != 0, (cudaStream_t)stream});
 }

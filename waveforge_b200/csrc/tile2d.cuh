@@ -94,52 +94,6 @@ struct TileSmem {
   unsigned bmax[3];
 };
 
-// The Ex, Ey, Hz region of the next tile a persistent CTA will run, staged in
-// shared memory by asynchronous copies while the current tile computes.
-template <class C>
-struct TileBuf {
-  alignas(16) float f[3][C::RH][C::RW];
-};
-
-// Where the next tile's region lies: its first domain row / column and the
-// number of region rows / columns inside the domain (the rest is zero-filled).
-struct TileNext {
-  const float *ex, *ey, *hz;
-  int ri0, rj0, RHa, RWa, ny;
-};
-
-__device__ __forceinline__ unsigned smem_addr32(const void* p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-// One 4-byte asynchronous global -> shared copy; valid = false writes a zero
-// and reads nothing (source size 0).
-__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_addr32(dst)), "l"(src),
-               "r"(valid ? 4 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// Every thread copies the cells it will own in the next tile (the same cell
-// map as the register load of tile2d), then commits the group.
-template <class C>
-__device__ __forceinline__ void tile_prefetch(const TileNext& Q, TileBuf<C>& B) {
-  constexpr int R = C::R, V = C::V, N = C::N;
-  const int c0 = (threadIdx.x & 31) * V, r0 = (threadIdx.x >> 5) * R;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    const int r = r0 + i / V, cc = c0 + i % V;
-    const bool valid = r < Q.RHa && cc < Q.RWa;
-    const long long g = valid ? (long long)(Q.ri0 + r) * Q.ny + (Q.rj0 + cc) : 0;
-    cp_async4(&B.f[0][r][cc], Q.ex + g, valid);
-    cp_async4(&B.f[1][r][cc], Q.ey + g, valid);
-    cp_async4(&B.f[2][r][cc], Q.hz + g, valid);
-  }
-  cp_async_commit();
-}
-
 // V consecutive floats to / from shared memory with one vector access (the
 // rows of TileSmem are 16-byte aligned and a lane's columns start at lane*V).
 template <int V>
@@ -398,17 +352,9 @@ __device__ __forceinline__ void tile2d_steps(const Tile2D& P, TileCtx& T, TileSm
   }
 }
 
-struct NoPrefetch {
-  __device__ void operator()() const {}
-};
-
-// PF: the tile's Ex, Ey, Hz region is already in B (staged by tile_prefetch
-// and waited for by the caller); once every thread holds its cells the routine
-// calls stage_next(), which may stage the next tile into B while this one
-// computes.
-template <class C, bool MAT, bool FDIV, bool PF = false, class Next = NoPrefetch>
+template <class C, bool MAT, bool FDIV>
 __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int step0, int k,
-                       TileSmem<C>& S, TileBuf<C>* B = nullptr, const Next& stage_next = Next{}) {
+                       TileSmem<C>& S) {
   constexpr int R = C::R, V = C::V, N = C::N;
   const int nx = P.nx, ny = P.ny;
   TileCtx T;
@@ -467,20 +413,13 @@ __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int 
     const int r = r0 + i / V, cc = c0 + i % V;
     ex[i] = ey[i] = hz[i] = 0.f;
     ca[i] = cb[i] = 0.f;
-    if (PF) {  // zero-filled outside the domain by the staging copies
-      ex[i] = B->f[0][r][cc];
-      ey[i] = B->f[1][r][cc];
-      hz[i] = B->f[2][r][cc];
-    }
     if (r < T.RHa && cc < T.RWa) {
       const long long g = (long long)(ri0 + r) * ny + (rj0 + cc);
       // state through L2 only: a persistent kernel may run a later pass of
       // the same solve on this SM, whose L1 can still hold older lines
-      if (!PF) {
-        ex[i] = __ldcg(P.ex_in + g);
-        ey[i] = __ldcg(P.ey_in + g);
-        hz[i] = __ldcg(P.hz_in + g);
-      }
+      ex[i] = __ldcg(P.ex_in + g);
+      ey[i] = __ldcg(P.ey_in + g);
+      hz[i] = __ldcg(P.hz_in + g);
       if (MAT) {
         ca[i] = __ldg(P.ca + g);
         cb[i] = __ldg(P.cb + g);
@@ -488,8 +427,6 @@ __device__ void tile2d(const Tile2D& P, int ci0, int ci1, int cj0, int cj1, int 
     }
   }
   __syncthreads();
-  // every thread holds its cells: B may take the next tile
-  if constexpr (PF) stage_next();
   T.nh = S.nh;
   T.ne = S.ne;
   T.np = min(S.np, kMaxLocalProbe);
