@@ -357,12 +357,16 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
     // Nx - 2 is read below, but no plane is issued then) unless the Mur code
     // reads plane f's old H, then after barrier C
     if (!face && tid == 0 && f + kRing <= plast) issue(f + kRing);
-    // Interior column block, interior plane, no sources / probes / check: every
-    // neighbour exists, so the update runs straight-line; halo threads compute
-    // too and only core threads store.
-    if (!LISTS && !face_blk && f >= ia && f >= 1 && f + 2 < nx) {
-     auto fastp = [&](auto s_tag) {
+    // Interior plane, no sources / probes / check: the update runs with the
+    // ring slots fixed at compile time; halo threads compute too and only
+    // core threads store.  In a column block off every face (FB false) every
+    // neighbour exists, so it is straight-line; a block on a j or k face (FB)
+    // keeps each cell's neighbour tests as selects and corrects its face
+    // cells in place between the Faraday and the Ampere halves.
+    if (!LISTS && f >= ia && f >= 1 && f + 2 < nx && (!face_blk || lite_ok)) {
+     auto fastp = [&](auto s_tag, auto fb_tag) {
       constexpr int SF = decltype(s_tag)::value;  // f & 3
+      constexpr bool FB = decltype(fb_tag)::value;
       const float* R = raw0 + ((SF + 1) & (kRing - 1)) * kSlotF;
       const float* R1 = raw0 + ((SF + 2) & (kRing - 1)) * kSlotF;
       const float ex = R[0], ey = cey, ez = cez;
@@ -370,34 +374,85 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       const float ex_k = R[1], ey_k = R[kTileF + 1];
       const float ey_i = R1[kTileF], ez_i = R1[2 * kTileF];
       float vx = R[3 * kTileF], vy = R[4 * kTileF], vz = R[5 * kTileF];
-      vx = fadd(vx, fmul(dh, fsub(dv<FDIV>(fsub(ey_k, ey), dz, rdz), dv<FDIV>(fsub(ez_j, ez), dy, rdy))));
-      vy = fadd(vy, fmul(dh, fsub(dv<FDIV>(fsub(ez_i, ez), dx, rdx), dv<FDIV>(fsub(ex_k, ex), dz, rdz))));
-      vz = fadd(vz, fmul(dh, fsub(dv<FDIV>(fsub(ex_j, ex), dy, rdy), dv<FDIV>(fsub(ey_i, ey), dx, rdx))));
+      {
+        const float nx_ = fadd(vx, fmul(dh, fsub(dv<FDIV>(fsub(ey_k, ey), dz, rdz), dv<FDIV>(fsub(ez_j, ez), dy, rdy))));
+        const float ny_ = fadd(vy, fmul(dh, fsub(dv<FDIV>(fsub(ez_i, ez), dx, rdx), dv<FDIV>(fsub(ex_k, ex), dz, rdz))));
+        const float nz_ = fadd(vz, fmul(dh, fsub(dv<FDIV>(fsub(ex_j, ex), dy, rdy), dv<FDIV>(fsub(ey_i, ey), dx, rdx))));
+        vx = (!FB || cjk) ? nx_ : vx;
+        vy = (!FB || ck) ? ny_ : vy;   // p < nx - 1 holds on these planes
+        vz = (!FB || cj) ? nz_ : vz;
+      }
       float* H = hc0 + ((SF + 1) & 1) * kHcSetF;
       H[0] = vx;
       H[kHcF] = vy;
       H[2 * kHcF] = vz;
-      // Ampere of plane f from the curl-updated (= final) H of plane f
+      float hxF = hcur.x, hyF = hcur.y, hzF = hcur.z;
+      if constexpr (FB) {
+        // Mur y and z faces of plane f, in place (as the general face path):
+        // face cells read hc(f) and plane f's old H, a barrier, then write
+        // their final H over hc(f); plane f's slot is refilled after that
+        auto Ho = [&](int c, int ww, int ll) -> float {
+          return S.raw[SF][3 + c][ww * kBoxK + ll + cofs];
+        };
+        auto Hc = [&](int c, int ww, int ll) -> float { return S.hc[SF & 1][c][ww][ll]; };
+        auto yfx = [&](int ww, int ll) -> float {
+          const int g = j0 + ww;
+          if (g == 0 && ww + 1 < kTJ) return fadd(Ho(0, ww + 1, ll), fmul(my, fsub(Hc(0, ww + 1, ll), Ho(0, ww, ll))));
+          if (g == ny - 1 && ww >= 1) return fadd(Ho(0, ww - 1, ll), fmul(my, fsub(Hc(0, ww - 1, ll), Ho(0, ww, ll))));
+          return Hc(0, ww, ll);
+        };
+        if (on_face) {
+          if (gj == 0 && w + 1 < kTJ) {
+            hxF = fadd(Ho(0, w + 1, lane), fmul(my, fsub(Hc(0, w + 1, lane), Ho(0, w, lane))));
+            hzF = fadd(Ho(2, w + 1, lane), fmul(my, fsub(Hc(2, w + 1, lane), Ho(2, w, lane))));
+          } else if (gj == ny - 1 && w >= 1) {
+            hxF = fadd(Ho(0, w - 1, lane), fmul(my, fsub(Hc(0, w - 1, lane), Ho(0, w, lane))));
+            hzF = fadd(Ho(2, w - 1, lane), fmul(my, fsub(Hc(2, w - 1, lane), Ho(2, w, lane))));
+          }
+          if (zf_on && in) {
+            if (gk == 0 && lane + 1 < kTK) {
+              hxF = fadd(Ho(0, w, lane + 1), fmul(mz, fsub(yfx(w, lane + 1), Ho(0, w, lane))));
+              hyF = fadd(Ho(1, w, lane + 1), fmul(mz, fsub(Hc(1, w, lane + 1), Ho(1, w, lane))));
+            } else if (gk == nz - 1 && lane >= 1) {
+              hxF = fadd(Ho(0, w, lane - 1), fmul(mz, fsub(yfx(w, lane - 1), Ho(0, w, lane))));
+              hyF = fadd(Ho(1, w, lane - 1), fmul(mz, fsub(Hc(1, w, lane - 1), Ho(1, w, lane))));
+            }
+          }
+        }
+        __syncthreads();  // every correction has read what it needs
+        if (on_face) {
+          S.hc[SF & 1][0][w][lane] = hxF;
+          S.hc[SF & 1][1][w][lane] = hyF;
+          S.hc[SF & 1][2][w][lane] = hzF;
+        }
+        __syncthreads();  // C: final H of plane f visible; plane f's slot unread
+        if (tid == 0 && f + kRing <= plast) issue(f + kRing);
+      }
+      // Ampere of plane f from the final H of plane f
       const float* N = hc0 + (SF & 1) * kHcSetF;
       const float hz_j = N[2 * kHcF - kTK], hx_j = N[-kTK];
       const float hy_k = N[kHcF - 1], hx_k = N[-1];
-      const float hxF = hcur.x, hyF = hcur.y, hzF = hcur.z;
       const float t1 = fsub(dv<FDIV>(fsub(hzF, hz_j), dy, rdy), dv<FDIV>(fsub(hyF, hy_k), dz, rdz));
       const float t2 = fsub(dv<FDIV>(fsub(hxF, hx_k), dz, rdz), dv<FDIV>(fsub(hzF, hprev.z), dx, rdx));
       const float t3 = fsub(dv<FDIV>(fsub(hyF, hprev.y), dx, rdx), dv<FDIV>(fsub(hxF, hx_j), dy, rdy));
-      const float exn = MAT ? fadd(fmul(cca, ecur.x), fmul(ccb, t1)) : fadd(ecur.x, fmul(de, t1));
-      const float eyn = MAT ? fadd(fmul(cca, ecur.y), fmul(ccb, t2)) : fadd(ecur.y, fmul(de, t2));
+      float exn = MAT ? fadd(fmul(cca, ecur.x), fmul(ccb, t1)) : fadd(ecur.x, fmul(de, t1));
+      float eyn = MAT ? fadd(fmul(cca, ecur.y), fmul(ccb, t2)) : fadd(ecur.y, fmul(de, t2));
       const float ezn = MAT ? fadd(fmul(cca, ecur.z), fmul(ccb, t3)) : fadd(ecur.z, fmul(de, t3));
+      if (FB) {  // f >= 1 here, so only the j and k tests remain
+        exn = (gj >= 1 && gk >= 1) ? exn : ecur.x;
+        eyn = gk >= 1 ? eyn : ecur.y;
+      }
+      const float ezf = (!FB || gj >= 1) ? ezn : ecur.z;
       if (core) {
         const unsigned o = (unsigned)f * PS32 + colg32;
         P.out[0][o] = exn;
         P.out[1][o] = eyn;
-        P.out[2][o] = ezn;
+        P.out[2][o] = ezf;
         P.out[3][o] = hxF;
         P.out[4][o] = hyF;
         P.out[5][o] = hzF;
       }
-      hprev = hcur;
+      hprev = F3{hxF, hyF, hzF};
       ecur = F3{ex, ey, ez};
       hcur = F3{vx, vy, vz};
       if (MAT) {
@@ -407,11 +462,20 @@ __global__ void __launch_bounds__(kTJ * kTK, 2) k3d_tma(const __grid_constant__ 
       cey = ey_i;
       cez = ez_i;
      };
-      switch (f & 3) {
-        case 0: fastp(std::integral_constant<int, 0>{}); break;
-        case 1: fastp(std::integral_constant<int, 1>{}); break;
-        case 2: fastp(std::integral_constant<int, 2>{}); break;
-        default: fastp(std::integral_constant<int, 3>{}); break;
+      if (face_blk) {
+        switch (f & 3) {
+          case 0: fastp(std::integral_constant<int, 0>{}, std::true_type{}); break;
+          case 1: fastp(std::integral_constant<int, 1>{}, std::true_type{}); break;
+          case 2: fastp(std::integral_constant<int, 2>{}, std::true_type{}); break;
+          default: fastp(std::integral_constant<int, 3>{}, std::true_type{}); break;
+        }
+      } else {
+        switch (f & 3) {
+          case 0: fastp(std::integral_constant<int, 0>{}, std::false_type{}); break;
+          case 1: fastp(std::integral_constant<int, 1>{}, std::false_type{}); break;
+          case 2: fastp(std::integral_constant<int, 2>{}, std::false_type{}); break;
+          default: fastp(std::integral_constant<int, 3>{}, std::false_type{}); break;
+        }
       }
       continue;
     }
