@@ -20,10 +20,10 @@
 // boundary); lanes read column lane + (k0 - 1 - floor4(k0 - 1)).
 // Curl-updated H of planes f and f+1 live in shared rows for the Mur faces and
 // the Ampere neighbours (the final H of plane f too, on x-face planes).
-// Column blocks that touch no domain face run interior planes straight-line
-// (no neighbour tests; ring slots fixed at compile time; halo threads compute
-// and do not store); blocks on a j or k face correct their face cells in
-// place.  Every mbarrier wait is bounded: after the limit the CTA records
+// Interior planes run with the ring slots fixed at compile time (halo threads
+// compute and do not store): straight-line in column blocks that touch no
+// domain face, with the neighbour tests as selects in blocks on a j or k face,
+// whose face cells correct H in place between the Faraday and Ampere halves.  Every mbarrier wait is bounded: after the limit the CTA records
 // WF_E_TIMEOUT, waits (bounded) for the copies it still has in flight, and
 // stops.
 #pragma once
