@@ -878,9 +878,9 @@ static int stream_seg_len(int nx, int ny, int nz, int rows) {
 // takes the total spread over the resident slots plus about one block's
 // length of tail.  Pick the segment count that minimises
 // blocks x (L + 2) / slots + (L + 2), with at least 22 planes per segment.
-// It picks 26 on a 256^3 volume and on 8 x 128^3; a sweep of lengths 16..64
-// puts both within 2 % of the best length (22 and 32), where the former
-// minimum of 16 planes lost 4 % at 256^3.
+// It picks 26 on a 256^3 volume and on 8 x 128^3, within 0.2 % of the best
+// length of a sweep over 16..64 on both; the former minimum of 16 planes lost
+// 4 % at 256^3.
 template <bool MAT, bool FDIV>
 static int tma_seg_len(int nx, int ny, int nz, int nb) {
   int dev = 0, nsm = 148, per_sm = 2;
